@@ -1,0 +1,342 @@
+"""Benchmark of the GSO docking step on B200 (scored poses/s and GSO steps/s).
+
+One bench step = one GSO step over every glowworm of the workload (rescore moved poses,
+luciferin, neighbour selection, movement).  Defaults: the mixed-precision single complex
+(receptor 3002 atoms, ligand 1274 atoms, 10+10 ANM modes, 402 swarms x 200 glowworms), 3
+warm-up steps + 97 timed steps = the workload's 100 GSO steps.  The plain FP64 kernels run the
+same steps from the same start for the mixed-vs-FP64 ratio.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c1]
+
+N > 1 (torchrun): every rank runs its own replica of the workload on its GPU (the swarms of
+the reference shard with no data exchange); value = all ranks' scored poses / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    "c0": dict(workload="single complex, plain FP64", complexes=[(757, 481, 130)], precision="fp64", steps=100),
+    "c1": dict(workload="single complex, mixed precision", complexes=[(3002, 1274, 402)], precision="mixed",
+               steps=100),
+    "c2": dict(workload="8 complexes batched, mixed precision",
+               complexes=[(757, 481, 130), (2039, 1440, 271), (2516, 1061, 298), (2030, 1256, 294),
+                          (3052, 1658, 336), (6058, 1138, 558), (6032, 1766, 695), (6143, 633, 620)],
+               precision="mixed", steps=100),
+    "c3": dict(workload="large receptor, mixed precision", complexes=[(17307, 1125, 1245)], precision="mixed",
+               steps=50),
+}
+G = 200
+METRIC = "scored poses/s and GSO steps/s on 1 B200, mixed vs FP64 at <=1e-5 rel energy err"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def make_complexes(cfg, seed0=100):
+    import sparkledock_b200 as sd
+    return [sd.SyntheticComplex(nr, nl, s, G, 10, 10, seed=seed0 + i) for i, (nr, nl, s) in enumerate(cfg["complexes"])]
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.p:
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+                self.out, _ = self.p.communicate()
+
+    def summary(self):
+        rows = [r.split(",") for r in (self.out or "").strip().splitlines() if r.count(",") >= 8]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k]})
+        loaded = sorted(sm)[len(sm) // 2:] if sm else []
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+def run_gpu(cfg, prec_name, steps, warmup, device, flush, seed=0):
+    """Device-timed run: draws resident in HBM, per-step CUDA events on the context stream,
+    L2 flushed (256 MB write) between timed steps outside the events."""
+    import torch
+    import sparkledock_b200 as sd
+    prec = {"mixed": sd.SD_PREC_MIXED, "fp64": sd.SD_PREC_FP64, "fp64_ref": sd.SD_PREC_FP64_REF}[prec_name]
+    cxs = make_complexes(cfg)
+    tables = sd.synthetic_tables(3)
+    total = warmup + steps
+    dk = sd.Docking(cxs, tables, precision=prec, device=device)
+    for i, c in enumerate(cxs):
+        dk.init_state(i, c.poses)
+        dk.set_draws(i, sd.gso_draws(seed + i, c.n_swarms, total, c.n_glowworms))
+    stream = torch.cuda.ExternalStream(dk.stream, device=device)
+    dk.step(warmup, sync=True)
+    s0 = dk.stats()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            if flush is not None:
+                flush.zero_()
+            starts[k].record(stream)
+            dk.step(1, sync=False)
+            ends[k].record(stream)
+    torch.cuda.synchronize(device)
+    ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
+    s1 = dk.stats()
+    out = {"ms": ms, "scored": s1["scored_poses"] - s0["scored_poses"], "stats": s1, "ctx": dk, "cxs": cxs}
+    return out
+
+
+def run_e2e(cfg, steps, device, seed=0):
+    """Same metric through the C ABI with host buffers: per step the step's draws go host->device
+    from pinned memory and the new state (positions, scores, luciferin) comes back."""
+    import torch
+    import sparkledock_b200 as sd
+    from sparkledock_b200 import _abi
+    import ctypes as C
+    cxs = make_complexes(cfg)
+    tables = sd.synthetic_tables(3)
+    dk = sd.Docking(cxs, tables, precision=sd.SD_PREC_MIXED, device=device)
+    U = []
+    outs = []
+    for i, c in enumerate(cxs):
+        dk.init_state(i, c.poses)
+        u = sd.gso_draws(seed + i, c.n_swarms, steps, c.n_glowworms)
+        pin = torch.empty((steps, c.n_swarms, 1, c.n_glowworms), dtype=torch.float64).pin_memory()
+        pin.numpy()[:] = np.transpose(u, (1, 0, 2))[:, :, None, :]
+        U.append(pin)
+        pos = torch.empty((c.n_swarms, c.n_glowworms, c.pose_len), dtype=torch.float64).pin_memory()
+        sc = torch.empty((c.n_swarms, c.n_glowworms), dtype=torch.float64).pin_memory()
+        lu = torch.empty((c.n_swarms, c.n_glowworms), dtype=torch.float64).pin_memory()
+        outs.append((pos, sc, lu))
+    L = _abi.lib()
+    h2d = sum(c.n_swarms * c.n_glowworms * 8 for c in cxs)
+    d2h = sum(c.n_swarms * c.n_glowworms * (c.pose_len + 2) * 8 for c in cxs)
+    s0 = dk.stats()
+    stream = torch.cuda.ExternalStream(dk.stream, device=device)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    t0 = time.perf_counter()
+    for t in range(steps):
+        for i, c in enumerate(cxs):
+            up = U[i][t]
+            _abi.check(L.sd_set_draws(dk._ctx, i, C.cast(up.data_ptr(), _abi._dp), 1), "sd_set_draws")
+        _abi.check(L.sd_step(dk._ctx, 1, 0), "sd_step")
+        for i, c in enumerate(cxs):
+            pos, sc, lu = outs[i]
+            st = _abi.SwarmState()
+            st.pos = C.cast(pos.data_ptr(), _abi._dp)
+            st.scoring = C.cast(sc.data_ptr(), _abi._dp)
+            st.luciferin = C.cast(lu.data_ptr(), _abi._dp)
+            _abi.check(L.sd_get_state(dk._ctx, i, C.byref(st)), "sd_get_state")
+    e1.record(stream)
+    torch.cuda.synchronize(device)
+    wall = time.perf_counter() - t0
+    ms = e0.elapsed_time(e1)
+    s1 = dk.stats()
+    scored = s1["scored_poses"] - s0["scored_poses"]
+    dk.close()
+    return {"ms": ms, "wall_s": wall, "scored": scored, "h2d": h2d, "d2h": d2h}
+
+
+def cpu_reference_rate(cfg, budget_s=12.0, seed=0):
+    """The reference's own CPU scoring path (oracle/_ref: its compiled cdfire_calculate_dfire,
+    rotate and GSO helpers, OpenMP over swarms) on a bounded swarm sample; falls back to the
+    oracle's C restatement when the reference harness was not built."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import sparkledock_b200 as sd
+    from oracle_bind import OracleState, OracleSystem, oracle_step, ref, ref_available, ref_step
+    cores = os.cpu_count() or 1
+    nr, nl, S = cfg["complexes"][0]
+    sample_s = max(1, min(S, 2 * cores))
+    cx = sd.SyntheticComplex(nr, nl, sample_s, G, 10, 10, seed=100)
+    tables = sd.synthetic_tables(3)
+    osys = OracleSystem(cx, tables, cr_math=0)
+    st = OracleState(sample_s, G, cx.pose_len, cx.poses)
+    U = sd.gso_draws(seed, sample_s, 100, G)
+    kind = "reference" if ref_available() else "port"
+    if kind == "reference":
+        ref()
+    scored = 0
+    t0 = time.perf_counter()
+    steps = 0
+    while steps < 100:
+        before = st.moved.copy(), st.step.copy()
+        if kind == "reference":
+            scored += ref_step(osys, st, U[:, steps, :], cores)
+        else:
+            oracle_step(osys, st, U[:, steps, :], nthreads=cores)
+            scored += int(((before[0] == 1) | (before[1] == 0)).sum())
+        steps += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": scored / dt, "unit": "scored poses/s", "cores": cores, "kind": kind,
+            "sample": f"{sample_s} of {S} swarms x {G} glowworms, {steps} GSO steps from the start "
+                      f"({scored} poses rescored in {dt:.1f} s, wall clock, OpenMP over swarms)",
+            "steps_per_s_sample": steps / dt}
+
+
+def rank_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def reduce_max_sum(dist, t_ms, scored, device):
+    """max of times and sum of scored poses over ranks (identity for one rank)."""
+    if dist is None:
+        return t_ms, scored
+    import torch
+    t = torch.tensor([t_ms], dtype=torch.float64, device=device)
+    s = torch.tensor([float(scored)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(s, op=dist.ReduceOp.SUM)
+    return float(t.item()), int(s.item())
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=97)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c1", choices=sorted(CONFIGS))
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison runs")
+    ap.add_argument("--cpu-budget", type=float, default=12.0)
+    args = ap.parse_args()
+    cfg = CONFIGS[args.config]
+    rank, world, local = rank_env()
+    config = {"workload": cfg["workload"], "complexes": [list(c) for c in cfg["complexes"]], "glowworms": G,
+              "anm_modes": [10, 10], "gso_steps": args.warmup + args.steps, "scoring": "dfire",
+              "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{args.gpus}"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        cb = cpu_reference_rate(cfg, args.cpu_budget)
+        line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "scored poses/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+                "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": cb["value"], "unit": "scored poses/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        dist_mod.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        dist = dist_mod
+    device = local if world > 1 else 0
+    torch.cuda.set_device(device)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(device)
+
+    barrier()
+    with Clocks(device) as clk:
+        run = run_gpu(cfg, cfg["precision"], args.steps, args.warmup, device, flush)
+    barrier()
+    t_ms, scored = reduce_max_sum(dist, sum(run["ms"]), run["scored"], device)
+    value = scored / (t_ms / 1e3)
+    stats = run["stats"]
+    run["ctx"].close()
+
+    extra = {}
+    if not args.no_fp64 and cfg["precision"] == "mixed":
+        for pname in ("fp64", "fp64_ref"):
+            r = run_gpu(cfg, pname, args.steps, args.warmup, device, flush)
+            tm, sc = reduce_max_sum(dist, sum(r["ms"]), r["scored"], device)
+            r["ctx"].close()
+            extra[pname] = {"value": sc / (tm / 1e3), "ms_per_step": tm / args.steps,
+                            "steps_per_s": args.steps / (tm / 1e3), "scored_poses": sc}
+    e2e = run_e2e(cfg, args.steps, device)
+    et, es = reduce_max_sum(dist, e2e["ms"], e2e["scored"], device)
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    peaks, peak_src = measured_peaks()
+    clocks = clk.summary()
+    # algorithmic work: 8 flops per receptor-ligand pair inside the 15 A cutoff (distance:
+    # 3 sub + 3 mul + 2 add); P_cut counted by the kernel
+    pairs = stats.get("pairs_in_cutoff", None)
+    fp32_peak = 148 * 128 * 2 * (peaks.get("sm_max_mhz", 1965.0) * 1e6) / 1e12
+    line = {
+        "metric": METRIC, "value": value, "unit": "scored poses/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "steps_per_s": args.steps / (t_ms / 1e3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 pairs, f64 GSO",
+        "data": "synthetic (seeded globules, N(0,1) DFIRE table)", "config": config,
+        "gpu_launches": 2 * args.steps,
+        "e2e": {"value": es / (et / 1e3), "unit": "scored poses/s", "h2d_bytes_per_step": e2e["h2d"],
+                "d2h_bytes_per_step": e2e["d2h"], "wall_s": e2e["wall_s"]},
+        "clocks": clocks,
+        "mixed_vs_fp64": {k: {**v, "speedup_mixed": value / v["value"]} for k, v in extra.items()},
+        "edge_counts": {k: stats[k] for k in ("pairs_fallback", "edge_d2_zero", "edge_d2_cutoff", "edge_u_zero",
+                                              "edge_shortfall")},
+    }
+    if pairs:
+        line["roofline"] = {"bound": "fp32", "achieved": 8.0 * pairs / (t_ms / 1e3) / 1e12, "peak": fp32_peak,
+                            "unit": "TFLOP/s", "frac": 8.0 * pairs / (t_ms / 1e3) / 1e12 / fp32_peak, "traffic": None,
+                            "peak_source": "nominal FP32 vector pipe at the measured max SM clock"}
+    if rank == 0 and world == 1:
+        try:
+            line["cpu_baseline"] = {k: v for k, v in cpu_reference_rate(cfg, args.cpu_budget).items()
+                                    if k in ("value", "unit", "cores", "kind", "sample")}
+        except Exception as e:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+    print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

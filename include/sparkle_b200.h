@@ -1,0 +1,207 @@
+/*
+ * sparkle_b200.h — C ABI of the B200 GSO docking path.
+ *
+ * This boundary replaces the reference's hot-path entry points:
+ *
+ *   prepare_gso_tasks(SwarmCenters&, Complex& rec, Complex& lig, FastDifire&, int seed,
+ *                     double step_t, double step_r, bool use_anm, double step_nm,
+ *                     int anm_rec, int anm_lig, bool local_min, int swarms, int G,
+ *                     int rank, int size)
+ *       source/dock/include/prepare_gso_tasks.h:8-11, body source/dock/src/prepare_gso_tasks.cc:1151-1256
+ *   cal_gso_tasks_gpu(...) / cal_gso_tasks_cpu(...)
+ *       source/dock/include/prepare_gso_tasks.h:18-26
+ *   cdfire_calculate_dfire(double* E, ..., int* rec_objects, int* lig_objects, FastDifire&,
+ *                          double* rec_xyz, double* lig_xyz, int Nr, int Nl, int g, int s)
+ *       source/dock/include/prepare_gso_tasks.h:36-40 (the scoring "plugin")
+ *
+ * Plain pointers and sizes only.  All pointers passed in are HOST pointers unless the
+ * argument name says otherwise; the context copies what it needs and owns its device
+ * memory for its lifetime.  Every call returns an int status (SD_OK == 0); a failing
+ * call leaves a message for sd_last_error().  Nothing here calls exit().
+ *
+ * Threading: one context is used by one host thread at a time; distinct contexts may be
+ * used concurrently.  Each context owns one CUDA stream on its device.
+ */
+#ifndef SPARKLE_B200_H
+#define SPARKLE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+/* ---- status codes ---- */
+#define SD_OK 0
+#define SD_ERR_ARG 1      /* bad argument (sizes, NULL, out-of-range type, ...) */
+#define SD_ERR_OOM 2      /* device or pinned allocation failed */
+#define SD_ERR_CUDA 3     /* a CUDA runtime call failed */
+#define SD_ERR_TIMEOUT 4  /* a bounded device wait gave up */
+#define SD_ERR_NUMERIC 5  /* NaN/Inf met in a pose or energy */
+#define SD_ERR_STATE 6    /* call out of order (no state set, draws exhausted, ...) */
+#define SD_ERR_NOTSUP 7   /* valid request this build does not support */
+
+/* ---- fixed model constants (reference source/dock/include/fastdfire.h:91-93, interface.h:30-35) ---- */
+#define SD_DFIRE_TYPES 168
+#define SD_DFIRE_BINS 20
+#define SD_MAX_MODES 10     /* DEFAULT_NMODES_REC / _LIG, prepare_gso_tasks.cc:23-24 */
+#define SD_LJ_TYPES 20
+#define SD_POSE_LEN(nm_rec, nm_lig) (7 + (nm_rec) + (nm_lig))
+
+/* scoring functions selectable by setup.json "scoring" */
+#define SD_SCORING_DFIRE 0   /* reference DFIRE (prepare_gso_tasks.cc:1522-1615) */
+#define SD_SCORING_PYDOCK 1  /* project-defined elec + LJ (no reference counterpart) */
+
+/* precision / algorithm of the pair stage */
+#define SD_PREC_FP64_REF 0   /* FP64, all Nr*Nl pairs, reference pair order: bit-exact energies */
+#define SD_PREC_FP64 1       /* FP64 with the cutoff cell culling; same order -> bit-exact */
+#define SD_PREC_MIXED 2      /* FP32 distances + compensated FP32 sums, FP64 near-boundary fallback */
+
+/* One receptor/ligand complex and its swarms.  Mirrors the fields of the reference's
+ * Complex (source/prep/include/complex.h:10-104: atom_coordinates, mask, modes, num_atoms)
+ * and the per-atom DFIRE objects made by get_docking_model (prepare_gso_tasks.cc:31-69). */
+typedef struct {
+  int n_rec, n_lig;
+  const double* rec_xyz;        /* [n_rec][3], receptor frame */
+  const double* lig_xyz;        /* [n_lig][3], ligand frame (rotation centre at origin) */
+  const int* rec_mask;          /* [n_rec], 0/1 ANM mask (get_nm_mask) */
+  const int* lig_mask;          /* [n_lig] */
+  int n_modes_rec, n_modes_lig; /* 0..SD_MAX_MODES */
+  const double* rec_modes;      /* [n_modes_rec][n_rec][3] */
+  const double* lig_modes;      /* [n_modes_lig][n_lig][3] */
+  const int* rec_dfire_type;    /* [n_rec], 0..167 */
+  const int* lig_dfire_type;    /* [n_lig], 0..167 */
+  const double* rec_charge;     /* [n_rec] partial charges (pyDock scoring; may be NULL for DFIRE) */
+  const double* lig_charge;     /* [n_lig] */
+  const int* rec_lj_type;       /* [n_rec], 0..19 (pyDock scoring; may be NULL for DFIRE) */
+  const int* lig_lj_type;       /* [n_lig] */
+  double lig_ref_point[3];      /* ligand reference point, ligand frame (minimum_volume_ellipsoid centre) */
+  int n_swarms, n_glowworms;
+} sd_complex_desc;
+
+/* Scoring tables shared by all complexes of a context. */
+typedef struct {
+  const double* dfire_energy;   /* [168*168*20], FastDifire.difire_energy layout [tR][tL][bin] */
+  const double* lj_eps;         /* [20] well depths (kcal/mol), pyDock scoring */
+  const double* lj_sigma;       /* [20] radii (A), pyDock scoring */
+} sd_tables;
+
+/* GSO parameters.  Defaults are the reference's Glowworm defaults (interface.h:9-26) and the
+ * literal 0.5 movement steps (prepare_gso_tasks.cc:783, :791-794). */
+typedef struct {
+  double rho, gamma, beta;
+  double initial_luciferin, initial_vision_range, max_vision_range;
+  int max_neighbors;
+  double translation_step, rotation_step, nmodes_step;
+} sd_gso_params;
+
+/* Per-glowworm state of one complex, structure-of-arrays, [S][G] row-major (swarm-major),
+ * the reference's SoA (prepare_gso_tasks.cc:370-409).  In sd_get_state any pointer may be
+ * NULL to skip that field; in sd_set_state all pointers are required. */
+typedef struct {
+  double* pos;                  /* [S][G][pose_len]: tx,ty,tz, qw,qx,qy,qz, ext_rec[], ext_lig[] */
+  double* scoring;              /* [S][G] last score of each glowworm */
+  double* luciferin;            /* [S][G] */
+  double* vision_range;         /* [S][G] */
+  int* step;                    /* [S][G] steps taken */
+  int* moved;                   /* [S][G] moved in the last step (rescored next step) */
+  int* nnei_len;                /* [S][G] neighbour count of the last step */
+  int* select;                  /* [S][G] neighbour chosen in the last step (self if none) */
+  double* ligand_reference_pose;/* [S][G][3] ligand reference point in the receptor frame */
+} sd_swarm_state;
+
+/* Counters of the rare paths, cumulative since context creation. */
+typedef struct {
+  long long scored_poses;       /* poses rescored (moved or first step) */
+  long long steps;              /* GSO steps taken */
+  long long pairs_fallback;     /* MIXED: pairs re-evaluated in FP64 near a bin or cutoff edge */
+  long long edge_d2_zero;       /* pairs at distance 0 (reference reads dist_to_bins[-1]) */
+  long long edge_d2_cutoff;     /* pairs at d^2 == 225 exactly (reference reads bin 20) */
+  long long edge_u_zero;        /* draws u <= 0 with neighbours (reference reads neighbors[-1]) */
+  long long edge_shortfall;     /* cumulative probability < u after all neighbours */
+  long long timeouts;           /* bounded device waits that gave up */
+  long long pairs_in_cutoff;    /* receptor-ligand pairs with d^2 <= 225 met while rescoring (GSO steps) */
+  long long pairs_evaluated;    /* pair distances computed after culling (GSO steps) */
+} sd_stats;
+
+typedef struct sd_ctx sd_ctx;
+
+/* ---- library ---- */
+const char* sd_last_error(void);          /* thread-local message of the last failing call */
+const char* sd_version(void);
+int sd_device_count(int* n);              /* visible CUDA devices (0 without a GPU) */
+void sd_gso_params_default(sd_gso_params* p);
+
+/* Reference random draws: u[s][t][g] ~ uniform_real_distribution<double>(0,1) over
+ * std::mt19937(seed) in swarm -> step -> glowworm order (prepare_gso_tasks.cc:411-427). */
+int sd_gso_draws(unsigned int seed, int n_swarms, int n_steps, int n_glowworms, double* u_out);
+
+/* ---- context ---- */
+int sd_ctx_create(const sd_complex_desc* complexes, int n_complexes, const sd_tables* tables,
+                  const sd_gso_params* params, int scoring, int precision, int device,
+                  sd_ctx** out);
+int sd_ctx_destroy(sd_ctx* ctx);
+int sd_ctx_stream(sd_ctx* ctx, void** cuda_stream_out);  /* the context's cudaStream_t */
+int sd_pose_len(const sd_ctx* ctx, int complex_idx, int* pose_len);
+
+/* Starting state: pos as given, luciferin/vision range from params, step = moved = 0
+ * (the reference's SoA initialisation, prepare_gso_tasks.cc:386-400). */
+int sd_init_state(sd_ctx* ctx, int complex_idx, const double* pos);
+int sd_set_state(sd_ctx* ctx, int complex_idx, const sd_swarm_state* st);
+int sd_get_state(sd_ctx* ctx, int complex_idx, sd_swarm_state* st);
+
+/* Random draws for the next n_steps of one complex, layout [S][n_steps][G]; replaces any
+ * draws not yet used. */
+int sd_set_draws(sd_ctx* ctx, int complex_idx, const double* u, int n_steps);
+
+/* n_steps GSO steps of every complex (pose -> score -> luciferin -> select -> move;
+ * reference step driver prepare_gso_task.cu:2745-2822, semantics of
+ * prepare_gso_tasks.cc:429-819).  Asynchronous on the context stream unless sync != 0. */
+int sd_step(sd_ctx* ctx, int n_steps, int sync);
+
+int sd_get_stats(sd_ctx* ctx, sd_stats* out);
+int sd_set_precision(sd_ctx* ctx, int precision);
+
+/* Score n arbitrary poses of one complex ([n][pose_len], host): score (reference sign
+ * convention, higher is better) and, if not NULL, raw energy and the ligand reference pose.
+ * DFIRE: energy = sum of table values, score = -(0.0157*energy - 4.7).
+ * PYDOCK: energy = E_elec + w_vdw*E_lj, score = -energy. */
+int sd_score_poses(sd_ctx* ctx, int complex_idx, const double* poses, int n, int precision,
+                   double* score_out, double* energy_out);
+
+/* Per-pair DFIRE bins of one pose (debug / parity): bins_out[i*n_lig + j] = table bin 0..19,
+ * -1 when d^2 > 225.  Receptor order i and ligand order j are the caller's. */
+int sd_dfire_bins(sd_ctx* ctx, int complex_idx, const double* pose, int precision, int* bins_out);
+
+/* PYDOCK only: energy and its gradient with respect to the 6 rigid coordinates and the ANM
+ * extents, grad_out[n][6 + n_modes_rec + n_modes_lig] =
+ *   dE/dt (3), dE/dw (3; left tangent rotation q <- exp(w/2) q), dE/de_rec, dE/de_lig.
+ * Project-defined (no reference counterpart). */
+int sd_pydock_grad(sd_ctx* ctx, int complex_idx, const double* poses, int n, int precision,
+                   double* energy_out, double* grad_out);
+
+/* ---- synthetic complexes (seeded), for tests and benchmarks ---- */
+typedef struct {
+  int n_rec, n_lig, n_swarms, n_glowworms, n_modes_rec, n_modes_lig;
+  unsigned long long seed;
+} sd_synth_spec;
+
+/* Sizes a caller must allocate for sd_synth_generate: all arrays of sd_complex_desc plus
+ * the starting poses [S][G][pose_len].  Returns the bytes of one contiguous buffer. */
+int sd_synth_buffer_size(const sd_synth_spec* spec, long long* bytes);
+/* Fills buf (sd_synth_buffer_size bytes) and points the fields of *desc into it; writes the
+ * starting poses to *poses_out (inside buf). */
+int sd_synth_generate(const sd_synth_spec* spec, void* buf, sd_complex_desc* desc,
+                      double** poses_out);
+/* Seeded synthetic DFIRE table N(0,1) [168*168*20] and LJ table [20] x2. */
+int sd_synth_tables(unsigned long long seed, double* dfire_energy, double* lj_eps,
+                    double* lj_sigma);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPARKLE_B200_H */

@@ -1,0 +1,214 @@
+"""sparkledock_b200 — B200-native glowworm swarm optimisation (GSO) docking step.
+
+Python view of the C ABI in include/sparkle_b200.h (libsparkle_b200.so).  It mirrors the
+reference's hot-path boundary, prepare_gso_tasks / cal_gso_tasks_gpu
+(source/dock/include/prepare_gso_tasks.h:8-26): a set of complexes with swarms of
+glowworms, the SoA glowworm state, the reference's random draws, one call per GSO step.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi
+from ._abi import (SD_PREC_FP64, SD_PREC_FP64_REF, SD_PREC_MIXED, SD_SCORING_DFIRE,  # noqa: F401
+                   SD_SCORING_PYDOCK, SparkleError, check, dptr, iptr)
+
+__all__ = ["SyntheticComplex", "synthetic_tables", "gso_draws", "GsoParams", "Docking",
+           "SD_PREC_FP64_REF", "SD_PREC_FP64", "SD_PREC_MIXED", "SD_SCORING_DFIRE",
+           "SD_SCORING_PYDOCK", "SparkleError", "device_count"]
+
+
+def device_count() -> int:
+    n = C.c_int(0)
+    check(_abi.lib().sd_device_count(C.byref(n)), "sd_device_count")
+    return n.value
+
+
+def gso_draws(seed: int, n_swarms: int, n_steps: int, n_glowworms: int) -> np.ndarray:
+    """The reference's draws u[s][t][g] (std::mt19937(seed), uniform_real_distribution(0,1))."""
+    out = np.empty((n_swarms, n_steps, n_glowworms), np.float64)
+    check(_abi.lib().sd_gso_draws(seed, n_swarms, n_steps, n_glowworms, dptr(out)), "sd_gso_draws")
+    return out
+
+
+def synthetic_tables(seed: int = 2024):
+    """Seeded N(0,1) DFIRE table [168*168*20] and a 20-type LJ (eps, sigma) table."""
+    t = np.empty(_abi.SD_DFIRE_TYPES * _abi.SD_DFIRE_TYPES * _abi.SD_DFIRE_BINS, np.float64)
+    e = np.empty(_abi.SD_LJ_TYPES, np.float64)
+    s = np.empty(_abi.SD_LJ_TYPES, np.float64)
+    check(_abi.lib().sd_synth_tables(seed, dptr(t), dptr(e), dptr(s)), "sd_synth_tables")
+    return t, e, s
+
+
+class SyntheticComplex:
+    """A seeded synthetic receptor/ligand pair with swarms and starting poses."""
+
+    def __init__(self, n_rec, n_lig, n_swarms, n_glowworms=200, n_modes_rec=10, n_modes_lig=10, seed=1):
+        spec = _abi.SynthSpec(n_rec, n_lig, n_swarms, n_glowworms, n_modes_rec, n_modes_lig, seed)
+        nbytes = C.c_longlong(0)
+        L = _abi.lib()
+        check(L.sd_synth_buffer_size(C.byref(spec), C.byref(nbytes)), "sd_synth_buffer_size")
+        self._buf = np.zeros(nbytes.value, np.uint8)
+        self.desc = _abi.ComplexDesc()
+        poses = _abi._dp()
+        check(L.sd_synth_generate(C.byref(spec), self._buf.ctypes.data_as(C.c_void_p), C.byref(self.desc),
+                                  C.byref(poses)), "sd_synth_generate")
+        self.spec = spec
+        self.n_rec, self.n_lig = n_rec, n_lig
+        self.n_swarms, self.n_glowworms = n_swarms, n_glowworms
+        self.n_modes_rec, self.n_modes_lig = n_modes_rec, n_modes_lig
+        self.pose_len = 7 + n_modes_rec + n_modes_lig
+        d = self.desc
+
+        def view(ptr, shape, dtype):
+            n = int(np.prod(shape))
+            if n == 0:
+                return np.zeros(shape, dtype)
+            ct = C.c_double if dtype == np.float64 else C.c_int
+            arr = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ct)), shape=(n,))
+            return arr.reshape(shape)
+
+        self.rec_xyz = view(d.rec_xyz, (n_rec, 3), np.float64)
+        self.lig_xyz = view(d.lig_xyz, (n_lig, 3), np.float64)
+        self.rec_mask = view(d.rec_mask, (n_rec,), np.int32)
+        self.lig_mask = view(d.lig_mask, (n_lig,), np.int32)
+        self.rec_modes = view(d.rec_modes, (n_modes_rec, n_rec, 3), np.float64)
+        self.lig_modes = view(d.lig_modes, (n_modes_lig, n_lig, 3), np.float64)
+        self.rec_type = view(d.rec_dfire_type, (n_rec,), np.int32)
+        self.lig_type = view(d.lig_dfire_type, (n_lig,), np.int32)
+        self.rec_charge = view(d.rec_charge, (n_rec,), np.float64)
+        self.lig_charge = view(d.lig_charge, (n_lig,), np.float64)
+        self.rec_lj = view(d.rec_lj_type, (n_rec,), np.int32)
+        self.lig_lj = view(d.lig_lj_type, (n_lig,), np.int32)
+        self.lig_ref = np.array(list(d.lig_ref_point), np.float64)
+        self.poses = view(poses, (n_swarms, n_glowworms, self.pose_len), np.float64)
+
+
+def GsoParams(**kw) -> _abi.GsoParams:
+    p = _abi.GsoParams()
+    _abi.lib().sd_gso_params_default(C.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+@dataclass
+class State:
+    pos: np.ndarray
+    scoring: np.ndarray
+    luciferin: np.ndarray
+    vision_range: np.ndarray
+    step: np.ndarray
+    moved: np.ndarray
+    nnei_len: np.ndarray
+    select: np.ndarray
+    ligand_reference_pose: np.ndarray
+
+    @staticmethod
+    def empty(S, G, pl):
+        return State(np.zeros((S, G, pl)), np.zeros((S, G)), np.zeros((S, G)), np.zeros((S, G)),
+                     np.zeros((S, G), np.int32), np.zeros((S, G), np.int32), np.zeros((S, G), np.int32),
+                     np.zeros((S, G), np.int32), np.zeros((S, G, 3)))
+
+    def as_c(self) -> _abi.SwarmState:
+        return _abi.SwarmState(dptr(self.pos), dptr(self.scoring), dptr(self.luciferin), dptr(self.vision_range),
+                               iptr(self.step), iptr(self.moved), iptr(self.nnei_len), iptr(self.select),
+                               dptr(self.ligand_reference_pose))
+
+    def copy(self) -> "State":
+        return State(*(np.array(getattr(self, f)) for f in self.__dataclass_fields__))
+
+
+class Docking:
+    """A context on one GPU holding complexes, their GSO state and the step graph."""
+
+    def __init__(self, complexes, tables, params=None, scoring=SD_SCORING_DFIRE, precision=SD_PREC_MIXED,
+                 device=0):
+        self._complexes = list(complexes)
+        descs = (_abi.ComplexDesc * len(self._complexes))(*[c.desc for c in self._complexes])
+        self._tables_np = tables
+        t = _abi.Tables(dptr(tables[0]), dptr(tables[1]), dptr(tables[2]))
+        self._params = params if params is not None else GsoParams()
+        ctx = C.c_void_p()
+        check(_abi.lib().sd_ctx_create(descs, len(self._complexes), C.byref(t), C.byref(self._params), scoring,
+                                       precision, device, C.byref(ctx)), "sd_ctx_create")
+        self._ctx = ctx
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            _abi.lib().sd_ctx_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def stream(self) -> int:
+        s = C.c_void_p()
+        check(_abi.lib().sd_ctx_stream(self._ctx, C.byref(s)), "sd_ctx_stream")
+        return s.value or 0
+
+    def init_state(self, ci: int, pos: np.ndarray):
+        pos = np.ascontiguousarray(pos, np.float64)
+        check(_abi.lib().sd_init_state(self._ctx, ci, dptr(pos)), "sd_init_state")
+
+    def set_state(self, ci: int, st: State):
+        cs = st.as_c()
+        check(_abi.lib().sd_set_state(self._ctx, ci, C.byref(cs)), "sd_set_state")
+
+    def get_state(self, ci: int) -> State:
+        c = self._complexes[ci]
+        st = State.empty(c.n_swarms, c.n_glowworms, c.pose_len)
+        cs = st.as_c()
+        check(_abi.lib().sd_get_state(self._ctx, ci, C.byref(cs)), "sd_get_state")
+        return st
+
+    def set_draws(self, ci: int, u: np.ndarray):
+        u = np.ascontiguousarray(u, np.float64)
+        check(_abi.lib().sd_set_draws(self._ctx, ci, dptr(u), u.shape[1]), "sd_set_draws")
+
+    def step(self, n: int = 1, sync: bool = True):
+        check(_abi.lib().sd_step(self._ctx, n, 1 if sync else 0), "sd_step")
+
+    def set_precision(self, precision: int):
+        check(_abi.lib().sd_set_precision(self._ctx, precision), "sd_set_precision")
+
+    def stats(self) -> dict:
+        s = _abi.Stats()
+        check(_abi.lib().sd_get_stats(self._ctx, C.byref(s)), "sd_get_stats")
+        return {f: getattr(s, f) for f, _ in _abi.Stats._fields_}
+
+    def score_poses(self, ci: int, poses: np.ndarray, precision: int = SD_PREC_MIXED):
+        poses = np.ascontiguousarray(poses, np.float64).reshape(-1, self._complexes[ci].pose_len)
+        n = poses.shape[0]
+        sc = np.empty(n)
+        en = np.empty(n)
+        check(_abi.lib().sd_score_poses(self._ctx, ci, dptr(poses), n, precision, dptr(sc), dptr(en)),
+              "sd_score_poses")
+        return sc, en
+
+    def dfire_bins(self, ci: int, pose: np.ndarray, precision: int = SD_PREC_MIXED) -> np.ndarray:
+        c = self._complexes[ci]
+        pose = np.ascontiguousarray(pose, np.float64)
+        out = np.empty((c.n_rec, c.n_lig), np.int32)
+        check(_abi.lib().sd_dfire_bins(self._ctx, ci, dptr(pose), precision, iptr(out)), "sd_dfire_bins")
+        return out
+
+    def pydock_grad(self, ci: int, poses: np.ndarray, precision: int = SD_PREC_MIXED):
+        c = self._complexes[ci]
+        poses = np.ascontiguousarray(poses, np.float64).reshape(-1, c.pose_len)
+        n = poses.shape[0]
+        e = np.empty(n)
+        g = np.empty((n, 6 + c.n_modes_rec + c.n_modes_lig))
+        check(_abi.lib().sd_pydock_grad(self._ctx, ci, dptr(poses), n, precision, dptr(e), dptr(g)),
+              "sd_pydock_grad")
+        return e, g

@@ -1,0 +1,132 @@
+// Internal declarations shared by the host runtime and the kernels.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include "../../include/sparkle_b200.h"
+
+#if defined(__CUDACC__)
+#include <cuda_runtime.h>
+#endif
+
+#define SD_TABLE_SIZE (SD_DFIRE_TYPES * SD_DFIRE_TYPES * SD_DFIRE_BINS)
+#define SD_ROW (SD_DFIRE_TYPES * SD_DFIRE_BINS)  /* 3360 */
+#define SD_CUTOFF2 225.0
+#define SD_MAX_COMPLEX 32
+#define SD_TILE 32              /* receptor atoms per tile (one warp lane each) */
+#define SD_MAX_LIG 6144         /* ligand atoms held in shared memory per pose */
+#define SD_MAX_REC 24576        /* receptor atoms (FP64 per-atom partials in shared memory) */
+#define SD_MAX_G 1024           /* glowworms per swarm (one thread each) */
+#define SD_CULL_MARGIN 0.05f    /* A, covers FP32 rounding of the conservative culling tests */
+
+namespace sd {
+
+// thread-local error message; returns code
+int fail(int code, const std::string& msg);
+void mvee_center(const double* p, int n, double tol, double* center);
+
+}  // namespace sd
+
+#if defined(__CUDACC__)
+namespace sd {
+
+// ---- device-side view of one complex (lives in device memory, read by every kernel) ----
+struct DevComplex {
+  int nr, nl, nmr, nml, S, G, pl;
+  int ntiles;           // receptor tiles of SD_TILE slots
+  int gbase, sbase;     // first global glowworm / swarm index of this complex
+  // receptor in tile order (slot = tile*32 + lane); padded slots have orig = -1
+  const int* r_orig;
+  const double* r_xyz;     // [nslots][3]
+  const double* r_modes;   // [nmr][nslots][3]
+  const int* r_mask;       // [nslots]
+  const int* r_row;        // [nslots] DFIRE row base tR*3360
+  const float4* r_tile;    // [ntiles] centre (rest frame) + radius
+  const float* r_q;        // [nslots] charge (pyDock)
+  const int* r_lj;         // [nslots] LJ type (pyDock)
+  // ligand in original order
+  const double* l_xyz;     // [nl][3]
+  const double* l_modes;   // [nml][nl][3]
+  const int* l_mask;
+  const int* l_col;        // [nl] tL*20
+  const float* l_q;
+  const int* l_lj;
+  float mnorm_r[SD_MAX_MODES], mnorm_l[SD_MAX_MODES];  // max per-atom mode norm (rounded up)
+  float lig_radius;        // max |l0_j| (rounded up)
+  float rec_span;          // max |r0_i - origin| (rounded up)
+  double lig_ref[3];
+  // GSO state [S][G]
+  double* pos;
+  double* scoring;
+  double* luciferin;
+  double* vision;
+  int* step;
+  int* moved;
+  int* nnei;
+  int* select;
+  double* ref;             // [S][G][3]
+  const double* draws;     // [S][draw_steps][G]
+  int draw_steps;
+  int draw_cursor;         // advanced by the GSO kernel (device copy authoritative)
+};
+
+struct StepCtl {
+  int count[2];            // items in work list [parity]
+  int grab[2];             // next item to grab in list [parity]
+  int parity;
+  int done_blocks;         // GSO blocks finished in this step
+  int step;
+  int pad;
+  unsigned long long stats[12];  // mirrors sd_stats order
+};
+
+enum { ST_SCORED = 0, ST_STEPS, ST_FALLBACK, ST_D2ZERO, ST_D2CUT, ST_UZERO, ST_SHORT, ST_TIMEOUT, ST_PAIRS, ST_EVALS };
+
+struct GsoParamsDev {
+  double rho, gamma, beta, max_vision, step_t, step_r, step_nm;
+  int max_neighbors;
+};
+
+// work item: complex index in the top 8 bits, local glowworm index below
+__host__ __device__ inline int wi_pack(int c, int local) { return (c << 24) | local; }
+__host__ __device__ inline int wi_complex(int w) { return (int)((unsigned)w >> 24); }
+__host__ __device__ inline int wi_local(int w) { return w & 0xFFFFFF; }
+
+struct ScoreLaunch {
+  const DevComplex* cplx;
+  StepCtl* ctl;
+  const int* work[2];
+  const double* table64;   // [SD_TABLE_SIZE + 32] zero padded
+  const float* table32;
+  const double* lj_eps;    // [20] pyDock
+  const double* lj_sigma;
+  double* energy_out;      // nullable [local glowworm] raw energies (stateless scoring)
+};
+
+struct GsoLaunch {
+  DevComplex* cplx;
+  StepCtl* ctl;
+  int* work[2];
+  const int* swarm_map;    // [total swarms] packed (complex, local swarm)
+  int nswarms_total;
+  int ncplx;               // <= 32 (the last CTA's first warp advances their draw cursors)
+  GsoParamsDev p;
+};
+
+// kernel launchers (sd_score.cu, sd_gso.cu)
+int score_launch(const ScoreLaunch& L, int precision, int scoring, int grid, int threads, size_t smem,
+                 cudaStream_t st);
+size_t score_smem_bytes(int precision, int scoring, int max_nr, int max_nl);
+const void* score_kernel_ptr(int precision, int scoring);
+int gso_launch(const GsoLaunch& L, int threads, cudaStream_t st);
+int bins_launch(const DevComplex* cplx, int c, const double* d_pose, int precision, int* d_bins, int nr, int nl,
+                int* d_fallback, cudaStream_t st);
+int pydock_grad_launch(const ScoreLaunch& L, int precision, int n, double* d_energy, double* d_grad, int grid,
+                       int threads, size_t smem, cudaStream_t st);
+size_t pydock_grad_smem_bytes(int max_nl);
+const void* pydock_grad_kernel_ptr(int precision);
+void set_key_thresholds(const double* t64);
+
+}  // namespace sd
+#endif  // __CUDACC__

@@ -1,0 +1,329 @@
+// Seeded synthetic docking systems: compact globular "proteins", DFIRE/LJ tables, ANM modes,
+// swarm centres and starting poses.  Stands in for the reference's PDB parsing + ANM + surface
+// sampling setup (source/dock/src/cal_anm.cc:61-219, :541-900), which the hot path only
+// consumes through Complex fields and SwarmCenters.pos.
+//
+// Globule: N points uniform in a sphere of radius 2.2*N^(1/3) A by rejection sampling with a
+// 3.0 A minimum separation (cell grid), centred on their centroid (as init_center_translate +
+// translate do, prepare: run_simulation.cc:58-59, :77-78).  Starting poses follow
+// calculate_start_pos (cal_anm.cc:833-896): Shoemake quaternion in the reference's component
+// order, N(0,1) ANM extents; the translation is the swarm centre plus N(0, 2 A) per axis.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "sd_internal.h"
+
+namespace sd {
+
+namespace {
+
+struct Rng {
+  std::mt19937_64 g;
+  explicit Rng(uint64_t s) : g(s) {}
+  double uniform() { return (double)(g() >> 11) * (1.0 / 9007199254740992.0); }  // [0,1)
+  double normal() {  // Box-Muller
+    double u1 = 1.0 - uniform();  // (0,1]
+    double u2 = uniform();
+    return std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+  }
+  int below(int n) { return (int)(uniform() * n); }
+};
+
+void globule(Rng& r, int n, double* xyz) {
+  const double R = 2.2 * std::cbrt((double)n);
+  const double dmin = 3.0, dmin2 = dmin * dmin;
+  const int nc = (int)std::ceil(2.0 * R / dmin) + 1;
+  std::vector<std::vector<int>> cells((size_t)nc * nc * nc);
+  auto cell_of = [&](double v) { return std::min(nc - 1, std::max(0, (int)((v + R) / dmin))); };
+  int placed = 0;
+  long long attempts = 0;
+  while (placed < n) {
+    double x = (2 * r.uniform() - 1) * R, y = (2 * r.uniform() - 1) * R, z = (2 * r.uniform() - 1) * R;
+    ++attempts;
+    if (x * x + y * y + z * z > R * R) continue;
+    int cx = cell_of(x), cy = cell_of(y), cz = cell_of(z);
+    bool ok = true;
+    for (int a = std::max(0, cx - 1); a <= std::min(nc - 1, cx + 1) && ok; ++a)
+      for (int b = std::max(0, cy - 1); b <= std::min(nc - 1, cy + 1) && ok; ++b)
+        for (int c = std::max(0, cz - 1); c <= std::min(nc - 1, cz + 1) && ok; ++c)
+          for (int k : cells[((size_t)a * nc + b) * nc + c]) {
+            double dx = xyz[k * 3] - x, dy = xyz[k * 3 + 1] - y, dz = xyz[k * 3 + 2] - z;
+            if (dx * dx + dy * dy + dz * dz < dmin2) {
+              ok = false;
+              break;
+            }
+          }
+    if (!ok) continue;
+    xyz[placed * 3] = x;
+    xyz[placed * 3 + 1] = y;
+    xyz[placed * 3 + 2] = z;
+    cells[((size_t)cx * nc + cy) * nc + cz].push_back(placed);
+    ++placed;
+  }
+  double c[3] = {0, 0, 0};
+  for (int i = 0; i < n; ++i)
+    for (int d = 0; d < 3; ++d) c[d] += xyz[i * 3 + d];
+  for (int d = 0; d < 3; ++d) c[d] /= n;
+  for (int i = 0; i < n; ++i)
+    for (int d = 0; d < 3; ++d) xyz[i * 3 + d] -= c[d];
+}
+
+// nm orthonormal 3N-vectors by modified Gram-Schmidt on Gaussian vectors
+void modes(Rng& r, int n, int nm, double* m) {
+  const size_t len = (size_t)n * 3;
+  for (int k = 0; k < nm; ++k) {
+    double* v = m + k * len;
+    for (size_t i = 0; i < len; ++i) v[i] = r.normal();
+    for (int p = 0; p < k; ++p) {
+      const double* u = m + p * len;
+      double dot = 0;
+      for (size_t i = 0; i < len; ++i) dot += u[i] * v[i];
+      for (size_t i = 0; i < len; ++i) v[i] -= dot * u[i];
+    }
+    double nrm = 0;
+    for (size_t i = 0; i < len; ++i) nrm += v[i] * v[i];
+    nrm = std::sqrt(nrm);
+    for (size_t i = 0; i < len; ++i) v[i] /= nrm;
+  }
+}
+
+void atoms(Rng& r, int n, int* type, double* charge, int* lj, int* mask) {
+  for (int i = 0; i < n; ++i) type[i] = r.below(SD_DFIRE_TYPES);
+  for (int i = 0; i < n; ++i) {
+    double u = r.uniform();
+    charge[i] = u < 0.05 ? -1.0 : u < 0.20 ? -0.5 : u < 0.80 ? 0.0 : u < 0.95 ? 0.5 : 1.0;
+  }
+  for (int i = 0; i < n; ++i) lj[i] = r.below(SD_LJ_TYPES);
+  // ANM mask: 1 for standard residues in the reference (get_nm_mask); a few 0s here
+  for (int i = 0; i < n; ++i) mask[i] = r.uniform() < 0.03 ? 0 : 1;
+}
+
+}  // namespace
+
+// Khachiyan's minimum-volume enclosing ellipsoid centre (the ligand reference point of
+// prepare_gso_tasks.cc:106-267 / :1196-1202, tolerance 0.01 as at :1196).  Only the diagonal
+// q_i^T X^-1 q_i is formed, O(N) per iteration.
+void mvee_center(const double* p, int n, double tol, double* center) {
+  std::vector<double> u(n, 1.0 / n);
+  double err = 1 + tol;
+  int it = 0;
+  while (err > tol && it < 100000) {
+    ++it;
+    double X[4][4] = {};
+    for (int i = 0; i < n; ++i) {
+      double q[4] = {p[i * 3], p[i * 3 + 1], p[i * 3 + 2], 1.0};
+      for (int a = 0; a < 4; ++a)
+        for (int b = 0; b < 4; ++b) X[a][b] += u[i] * q[a] * q[b];
+    }
+    // invert 4x4 by Gauss-Jordan
+    double A[4][8];
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 8; ++b) A[a][b] = b < 4 ? X[a][b] : (b - 4 == a ? 1.0 : 0.0);
+    for (int c = 0; c < 4; ++c) {
+      int piv = c;
+      for (int a = c + 1; a < 4; ++a)
+        if (std::fabs(A[a][c]) > std::fabs(A[piv][c])) piv = a;
+      for (int b = 0; b < 8; ++b) std::swap(A[c][b], A[piv][b]);
+      double d = A[c][c];
+      for (int b = 0; b < 8; ++b) A[c][b] /= d;
+      for (int a = 0; a < 4; ++a)
+        if (a != c) {
+          double f = A[a][c];
+          for (int b = 0; b < 8; ++b) A[a][b] -= f * A[c][b];
+        }
+    }
+    double mx = -1;
+    int j = 0;
+    for (int i = 0; i < n; ++i) {
+      double q[4] = {p[i * 3], p[i * 3 + 1], p[i * 3 + 2], 1.0}, m = 0;
+      for (int a = 0; a < 4; ++a)
+        for (int b = 0; b < 4; ++b) m += q[a] * A[a][4 + b] * q[b];
+      if (m > mx) {
+        mx = m;
+        j = i;
+      }
+    }
+    double step = (mx - 3 - 1.0) / ((3 + 1.0) * (mx - 1.0));
+    double e2 = 0;
+    for (int i = 0; i < n; ++i) {
+      double nu = (1.0 - step) * u[i] + (i == j ? step : 0.0);
+      e2 += (nu - u[i]) * (nu - u[i]);
+      u[i] = nu;
+    }
+    err = std::sqrt(e2);
+  }
+  for (int d = 0; d < 3; ++d) {
+    double c = 0;
+    for (int i = 0; i < n; ++i) c += p[i * 3 + d] * u[i];
+    center[d] = c;
+  }
+}
+
+}  // namespace sd
+
+namespace {
+struct Layout {
+  size_t rec_xyz, lig_xyz, rec_modes, lig_modes, rec_charge, lig_charge, poses;
+  size_t rec_mask, lig_mask, rec_type, lig_type, rec_lj, lig_lj, total;
+};
+Layout layout_of(const sd_synth_spec* s) {
+  Layout L;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = off;
+    off += (bytes + 255) & ~(size_t)255;
+    return o;
+  };
+  const size_t nr = s->n_rec, nl = s->n_lig, pl = SD_POSE_LEN(s->n_modes_rec, s->n_modes_lig);
+  L.rec_xyz = take(nr * 3 * 8);
+  L.lig_xyz = take(nl * 3 * 8);
+  L.rec_modes = take((size_t)s->n_modes_rec * nr * 3 * 8);
+  L.lig_modes = take((size_t)s->n_modes_lig * nl * 3 * 8);
+  L.rec_charge = take(nr * 8);
+  L.lig_charge = take(nl * 8);
+  L.poses = take((size_t)s->n_swarms * s->n_glowworms * pl * 8);
+  L.rec_mask = take(nr * 4);
+  L.lig_mask = take(nl * 4);
+  L.rec_type = take(nr * 4);
+  L.lig_type = take(nl * 4);
+  L.rec_lj = take(nr * 4);
+  L.lig_lj = take(nl * 4);
+  L.total = off;
+  return L;
+}
+bool spec_ok(const sd_synth_spec* s) {
+  return s && s->n_rec > 0 && s->n_lig > 0 && s->n_swarms > 0 && s->n_glowworms > 0 && s->n_modes_rec >= 0 &&
+         s->n_modes_rec <= SD_MAX_MODES && s->n_modes_lig >= 0 && s->n_modes_lig <= SD_MAX_MODES &&
+         s->n_rec <= 200000 && s->n_lig <= 200000;
+}
+}  // namespace
+
+extern "C" int sd_synth_buffer_size(const sd_synth_spec* spec, long long* bytes) {
+  if (!spec_ok(spec) || !bytes) return sd::fail(SD_ERR_ARG, "sd_synth_buffer_size: bad spec");
+  *bytes = (long long)layout_of(spec).total;
+  return SD_OK;
+}
+
+extern "C" int sd_synth_generate(const sd_synth_spec* s, void* buf, sd_complex_desc* d, double** poses_out) {
+  if (!spec_ok(s) || !buf || !d) return sd::fail(SD_ERR_ARG, "sd_synth_generate: bad arguments");
+  Layout L = layout_of(s);
+  char* b = (char*)buf;
+  double* rec_xyz = (double*)(b + L.rec_xyz);
+  double* lig_xyz = (double*)(b + L.lig_xyz);
+  double* rec_modes = (double*)(b + L.rec_modes);
+  double* lig_modes = (double*)(b + L.lig_modes);
+  double* rec_charge = (double*)(b + L.rec_charge);
+  double* lig_charge = (double*)(b + L.lig_charge);
+  double* poses = (double*)(b + L.poses);
+  int* rec_mask = (int*)(b + L.rec_mask);
+  int* lig_mask = (int*)(b + L.lig_mask);
+  int* rec_type = (int*)(b + L.rec_type);
+  int* lig_type = (int*)(b + L.lig_type);
+  int* rec_lj = (int*)(b + L.rec_lj);
+  int* lig_lj = (int*)(b + L.lig_lj);
+
+  sd::Rng rr(s->seed * 4 + 1), rl(s->seed * 4 + 2), rs(s->seed * 4 + 3);
+  sd::globule(rr, s->n_rec, rec_xyz);
+  sd::atoms(rr, s->n_rec, rec_type, rec_charge, rec_lj, rec_mask);
+  sd::modes(rr, s->n_rec, s->n_modes_rec, rec_modes);
+  sd::globule(rl, s->n_lig, lig_xyz);
+  sd::atoms(rl, s->n_lig, lig_type, lig_charge, lig_lj, lig_mask);
+  sd::modes(rl, s->n_lig, s->n_modes_lig, lig_modes);
+
+  memset(d, 0, sizeof *d);
+  d->n_rec = s->n_rec;
+  d->n_lig = s->n_lig;
+  d->rec_xyz = rec_xyz;
+  d->lig_xyz = lig_xyz;
+  d->rec_mask = rec_mask;
+  d->lig_mask = lig_mask;
+  d->n_modes_rec = s->n_modes_rec;
+  d->n_modes_lig = s->n_modes_lig;
+  d->rec_modes = rec_modes;
+  d->lig_modes = lig_modes;
+  d->rec_dfire_type = rec_type;
+  d->lig_dfire_type = lig_type;
+  d->rec_charge = rec_charge;
+  d->lig_charge = lig_charge;
+  d->rec_lj_type = rec_lj;
+  d->lig_lj_type = lig_lj;
+  sd::mvee_center(lig_xyz, s->n_lig, 0.01, d->lig_ref_point);
+  d->n_swarms = s->n_swarms;
+  d->n_glowworms = s->n_glowworms;
+
+  // swarm centres on a shell 10 A outside the receptor surface
+  double rmax = 0;
+  for (int i = 0; i < s->n_rec; ++i)
+    rmax = std::max(rmax, std::sqrt(rec_xyz[i * 3] * rec_xyz[i * 3] + rec_xyz[i * 3 + 1] * rec_xyz[i * 3 + 1] +
+                                    rec_xyz[i * 3 + 2] * rec_xyz[i * 3 + 2]));
+  const double shell = rmax + 10.0;
+  const int pl = SD_POSE_LEN(s->n_modes_rec, s->n_modes_lig);
+  const double PI = 3.14159265358979323846;
+  for (int sw = 0; sw < s->n_swarms; ++sw) {
+    double v[3], n2 = 0;
+    do {
+      n2 = 0;
+      for (int k = 0; k < 3; ++k) {
+        v[k] = rs.normal();
+        n2 += v[k] * v[k];
+      }
+    } while (n2 < 1e-12);
+    double nrm = std::sqrt(n2);
+    double c[3] = {v[0] / nrm * shell, v[1] / nrm * shell, v[2] / nrm * shell};
+    for (int g = 0; g < s->n_glowworms; ++g) {
+      double* p = poses + ((size_t)sw * s->n_glowworms + g) * pl;
+      for (int k = 0; k < 3; ++k) p[k] = c[k] + 2.0 * rs.normal();
+      double u1 = rs.uniform(), u2 = rs.uniform(), u3 = rs.uniform();
+      p[3] = std::sqrt(1 - u1) * std::sin(2 * PI * u2);
+      p[4] = std::sqrt(1 - u1) * std::cos(2 * PI * u2);
+      p[5] = std::sqrt(u1) * std::sin(2 * PI * u3);
+      p[6] = std::sqrt(u1) * std::cos(2 * PI * u3);
+      for (int k = 0; k < s->n_modes_rec + s->n_modes_lig; ++k) p[7 + k] = rs.normal();
+    }
+  }
+  if (poses_out) *poses_out = poses;
+  return SD_OK;
+}
+
+extern "C" int sd_synth_tables(unsigned long long seed, double* dfire, double* eps, double* sigma) {
+  sd::Rng r(seed * 4 + 0);
+  if (dfire)
+    for (size_t i = 0; i < (size_t)SD_DFIRE_TYPES * SD_DFIRE_TYPES * SD_DFIRE_BINS; ++i) dfire[i] = r.normal();
+  sd::Rng r2(seed * 4 + 7);
+  for (int i = 0; i < SD_LJ_TYPES; ++i) {
+    double e = 0.05 + 0.25 * r2.uniform();
+    double s = 2.8 + 1.4 * r2.uniform();
+    if (eps) eps[i] = e;
+    if (sigma) sigma[i] = s;
+  }
+  return SD_OK;
+}
+
+extern "C" int sd_gso_draws(unsigned int seed, int S, int steps, int G, double* out) {
+  if (S <= 0 || steps <= 0 || G <= 0 || !out) return sd::fail(SD_ERR_ARG, "sd_gso_draws: bad arguments");
+  // prepare_gso_tasks.cc:411-427: one engine, swarm -> step -> glowworm
+  std::uniform_real_distribution<double> distribution(0.0, 1.0);
+  std::mt19937 gen(seed);
+  for (int i = 0; i < S; i++)
+    for (int s = 0; s < steps; s++)
+      for (int j = 0; j < G; j++) out[(size_t)i * steps * G + (size_t)s * G + j] = distribution(gen);
+  return SD_OK;
+}
+
+extern "C" void sd_gso_params_default(sd_gso_params* p) {
+  if (!p) return;
+  p->rho = 0.4;
+  p->gamma = 0.6;
+  p->beta = 0.08;
+  p->initial_luciferin = 5.0;
+  p->initial_vision_range = 0.2;
+  p->max_vision_range = 5.0;
+  p->max_neighbors = 5;
+  p->translation_step = 0.5;
+  p->rotation_step = 0.5;
+  p->nmodes_step = 0.5;
+}

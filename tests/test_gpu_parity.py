@@ -1,0 +1,137 @@
+"""GPU parity of the DFIRE GSO path against the oracle, through the C ABI.
+
+Bars (written in the tests):
+  * FP64 modes: scores, energies, GSO state and every bin bit-identical to the oracle;
+  * MIXED: every bin bit-identical, |E_gpu - E_64| / max(|E_64|, 1) <= 1e-5 per pose, and the
+    GSO update bit-identical when fed the GPU's own scores (step-locked, every step).
+"""
+import numpy as np
+import pytest
+
+import sparkledock_b200 as sd
+from oracle_bind import OracleState, OracleSystem, oracle_bins, oracle_scores, oracle_step
+
+pytestmark = pytest.mark.gpu
+
+MIXED_TOL = 1e-5
+STATE_FIELDS = (("pos", "pos"), ("scoring", "scoring"), ("luciferin", "luciferin"),
+                ("vision_range", "vision"), ("step", "step"), ("moved", "moved"), ("nnei_len", "nnei"),
+                ("select", "select"), ("ligand_reference_pose", "ref"))
+
+
+def rel_err(a, b, floor=1.0):
+    return np.abs(np.asarray(a) - np.asarray(b)) / np.maximum(np.abs(b), floor)
+
+
+@pytest.fixture(scope="module")
+def c0():
+    # config-0 atom counts, few swarms so the oracle finishes in seconds
+    return sd.SyntheticComplex(757, 481, 3, 200, seed=7)
+
+
+def test_scores_all_precisions(c0, tables):
+    osys = OracleSystem(c0, tables)
+    poses = c0.poses.reshape(-1, c0.pose_len)[:240]
+    ref_sc, ref_en = oracle_scores(osys, poses)
+    with sd.Docking([c0], tables) as dk:
+        for prec in (sd.SD_PREC_FP64_REF, sd.SD_PREC_FP64):
+            sc, en = dk.score_poses(0, poses, prec)
+            assert np.array_equal(en, ref_en), f"precision {prec}: FP64 energies not bit-identical"
+            assert np.array_equal(sc, ref_sc)
+        sc, en = dk.score_poses(0, poses, sd.SD_PREC_MIXED)
+        assert rel_err(en, ref_en).max() <= MIXED_TOL
+        assert rel_err(sc, ref_sc).max() <= MIXED_TOL
+
+
+def test_bins_bit_exact(c0, tables):
+    osys = OracleSystem(c0, tables)
+    poses = c0.poses.reshape(-1, c0.pose_len)
+    with sd.Docking([c0], tables) as dk:
+        for k in (0, 17, 333):
+            ob, _, _, _, _ = oracle_bins(osys, poses[k])
+            assert (ob >= 0).sum() > 0
+            for prec in (sd.SD_PREC_FP64, sd.SD_PREC_MIXED):
+                gb = dk.dfire_bins(0, poses[k], prec)
+                assert np.array_equal(gb, ob), f"pose {k} precision {prec}: bins differ"
+
+
+def test_gso_trajectory_fp64_bit_exact(c0, tables):
+    steps = 25
+    U = sd.gso_draws(0, c0.n_swarms, steps, c0.n_glowworms)
+    osys = OracleSystem(c0, tables)
+    st = OracleState(c0.n_swarms, c0.n_glowworms, c0.pose_len, c0.poses)
+    with sd.Docking([c0], tables, precision=sd.SD_PREC_FP64) as dk:
+        dk.init_state(0, c0.poses)
+        dk.set_draws(0, U)
+        for t in range(steps):
+            oracle_step(osys, st, U[:, t, :])
+            dk.step(1)
+            g = dk.get_state(0)
+            for f, o in STATE_FIELDS:
+                assert np.array_equal(getattr(g, f), getattr(st, o)), f"step {t}: {f} differs"
+        stats = dk.stats()
+    assert stats["steps"] == steps
+    assert stats["edge_u_zero"] == 0 and stats["edge_shortfall"] == 0
+
+
+def test_gso_step_locked_mixed(c0, tables):
+    steps = 12
+    U = sd.gso_draws(1, c0.n_swarms, steps, c0.n_glowworms)
+    osys = OracleSystem(c0, tables)
+    st = OracleState(c0.n_swarms, c0.n_glowworms, c0.pose_len, c0.poses)
+    worst = 0.0
+    with sd.Docking([c0], tables, precision=sd.SD_PREC_MIXED) as dk:
+        for t in range(steps):
+            gs = sd.State(st.pos.copy(), st.scoring.copy(), st.luciferin.copy(), st.vision.copy(),
+                          st.step.copy(), st.moved.copy(), st.nnei.copy(), st.select.copy(), st.ref.copy())
+            dk.set_state(0, gs)
+            dk.set_draws(0, U[:, t:t + 1, :])
+            dk.step(1)
+            g = dk.get_state(0)
+            rescored = (st.moved == 1) | (st.step == 0)
+            # FP64 oracle energies of the rescored poses at the pre-step state
+            free = st.copy()
+            oracle_step(osys, free, U[:, t, :])
+            err = rel_err(g.scoring[rescored], free.scoring[rescored])
+            worst = max(worst, float(err.max()) if err.size else 0.0)
+            assert worst <= MIXED_TOL, f"step {t}: score error {worst:.3g}"
+            # the GSO update fed with the GPU's scores must be bit-identical
+            oracle_step(osys, st, U[:, t, :], score_override=g.scoring)
+            for f, o in STATE_FIELDS:
+                assert np.array_equal(getattr(g, f), getattr(st, o)), f"step {t}: {f} differs"
+
+
+def test_multi_complex_batch_fp64(tables):
+    cxs = [sd.SyntheticComplex(300, 200, 2, 50, seed=21), sd.SyntheticComplex(520, 140, 3, 32, seed=22),
+           sd.SyntheticComplex(180, 260, 1, 96, n_modes_rec=4, n_modes_lig=0, seed=23)]
+    steps = 6
+    Us = [sd.gso_draws(5 + i, c.n_swarms, steps, c.n_glowworms) for i, c in enumerate(cxs)]
+    osyss = [OracleSystem(c, tables) for c in cxs]
+    sts = [OracleState(c.n_swarms, c.n_glowworms, c.pose_len, c.poses) for c in cxs]
+    with sd.Docking(cxs, tables, precision=sd.SD_PREC_FP64) as dk:
+        for i, c in enumerate(cxs):
+            dk.init_state(i, c.poses)
+            dk.set_draws(i, Us[i])
+        for t in range(steps):
+            dk.step(1)
+            for i in range(len(cxs)):
+                oracle_step(osyss[i], sts[i], Us[i][:, t, :])
+                g = dk.get_state(i)
+                for f, o in STATE_FIELDS:
+                    assert np.array_equal(getattr(g, f), getattr(sts[i], o)), f"complex {i} step {t}: {f}"
+
+
+def test_errors_are_status_codes(c0, tables):
+    with sd.Docking([c0], tables) as dk:
+        with pytest.raises(sd.SparkleError) as e:
+            dk.step(1)  # no state yet
+        assert e.value.code == 6
+        dk.init_state(0, c0.poses)
+        with pytest.raises(sd.SparkleError) as e:
+            dk.step(1)  # no draws yet
+        assert e.value.code == 6
+        bad = c0.poses.copy()
+        bad[0, 0, 0] = np.nan
+        with pytest.raises(sd.SparkleError) as e:
+            dk.score_poses(0, bad.reshape(-1, c0.pose_len)[:2])
+        assert e.value.code == 5
