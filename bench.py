@@ -83,7 +83,7 @@ class Clocks:
         sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k]})
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
         loaded = sorted(sm)[len(sm) // 2:] if sm else []
         return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(rows)}
@@ -245,8 +245,17 @@ def main():
     ap.add_argument("--config", default="c1", choices=sorted(CONFIGS))
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison runs")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
+    ap.add_argument("--swarms", type=int, default=0, help="override the swarm count (profiling of a smaller case)")
+    ap.add_argument("--precision", default="", choices=["", "mixed", "fp64", "fp64_ref"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
-    cfg = CONFIGS[args.config]
+    cfg = dict(CONFIGS[args.config])
+    if args.swarms:
+        cfg["complexes"] = [(nr, nl, min(s, args.swarms)) for nr, nl, s in cfg["complexes"]]
+        cfg["workload"] += f" (swarms capped at {args.swarms})"
+    if args.precision:
+        cfg["precision"] = args.precision
     rank, world, local = rank_env()
     config = {"workload": cfg["workload"], "complexes": [list(c) for c in cfg["complexes"]], "glowworms": G,
               "anm_modes": [10, 10], "gso_steps": args.warmup + args.steps, "scoring": "dfire",
@@ -297,7 +306,10 @@ def main():
             r["ctx"].close()
             extra[pname] = {"value": sc / (tm / 1e3), "ms_per_step": tm / args.steps,
                             "steps_per_s": args.steps / (tm / 1e3), "scored_poses": sc}
-    e2e = run_e2e(cfg, args.steps, device)
+    if args.no_e2e:
+        e2e = {"ms": float("nan"), "wall_s": None, "scored": 0, "h2d": 0, "d2h": 0}
+    else:
+        e2e = run_e2e(cfg, args.steps, device)
     et, es = reduce_max_sum(dist, e2e["ms"], e2e["scored"], device)
 
     if rank != 0:
@@ -322,12 +334,15 @@ def main():
         "mixed_vs_fp64": {k: {**v, "speedup_mixed": value / v["value"]} for k, v in extra.items()},
         "edge_counts": {k: stats[k] for k in ("pairs_fallback", "edge_d2_zero", "edge_d2_cutoff", "edge_u_zero",
                                               "edge_shortfall")},
+        "per_scored_pose": {"pairs_in_cutoff": stats["pairs_in_cutoff"] / max(1, stats["scored_poses"]),
+                            "pairs_evaluated": stats["pairs_evaluated"] / max(1, stats["scored_poses"]),
+                            "pairs_brute_force": sum(nr * nl for nr, nl, _ in cfg["complexes"]) / len(cfg["complexes"])},
     }
     if pairs:
         line["roofline"] = {"bound": "fp32", "achieved": 8.0 * pairs / (t_ms / 1e3) / 1e12, "peak": fp32_peak,
                             "unit": "TFLOP/s", "frac": 8.0 * pairs / (t_ms / 1e3) / 1e12 / fp32_peak, "traffic": None,
                             "peak_source": "nominal FP32 vector pipe at the measured max SM clock"}
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.no_cpu:
         try:
             line["cpu_baseline"] = {k: v for k, v in cpu_reference_rate(cfg, args.cpu_budget).items()
                                     if k in ("value", "unit", "cores", "kind", "sample")}

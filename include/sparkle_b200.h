@@ -181,6 +181,14 @@ int sd_dfire_bins(sd_ctx* ctx, int complex_idx, const double* pose, int precisio
 int sd_pydock_grad(sd_ctx* ctx, int complex_idx, const double* poses, int n, int precision,
                    double* energy_out, double* grad_out);
 
+/* Result files of the reference GPU path (prepare_gso_task.cu:2838-2905): writes
+ * <dir>/swarm_<swarm_offset+s>/gso_<steps>.out for s in [0, n_swarms) from host state arrays
+ * ([S][G][pose_len] positions, [S][G] luciferin, neighbour counts, vision ranges, scores).
+ * Host only; creates the swarm directories. */
+int sd_write_gso_output(const char* dir, int swarm_offset, int n_swarms, int n_glowworms, int pose_len,
+                        int steps, const double* pos, const double* luciferin, const int* nnei_len,
+                        const double* vision_range, const double* scoring);
+
 /* ---- synthetic complexes (seeded), for tests and benchmarks ---- */
 typedef struct {
   int n_rec, n_lig, n_swarms, n_glowworms, n_modes_rec, n_modes_lig;

@@ -312,6 +312,40 @@ int setup_complex(sd_ctx* c, const sd_complex_desc& d, ComplexHost& h, int gbase
   if ((rc = upload(c, h, rq.data(), rq.size(), &D.r_q))) return rc;
   if ((rc = upload(c, h, rlj.data(), rlj.size(), &D.r_lj))) return rc;
 
+  // ligand chunks (spatial order) for the mixed-precision kernel
+  {
+    std::vector<int> lslots;
+    build_tiles(d.lig_xyz, d.n_lig, lslots);
+    D.nlchunks = (int)lslots.size() / SD_TILE;
+    std::vector<float4> lch(D.nlchunks);
+    for (int t = 0; t < D.nlchunks; ++t) {
+      double ctr[3] = {0, 0, 0};
+      int cnt = 0;
+      for (int l = 0; l < SD_TILE; ++l) {
+        const int j = lslots[t * SD_TILE + l];
+        if (j < 0) continue;
+        for (int k = 0; k < 3; ++k) ctr[k] += d.lig_xyz[(size_t)j * 3 + k];
+        ++cnt;
+      }
+      float cf[3];
+      for (int k = 0; k < 3; ++k) cf[k] = (float)(ctr[k] / std::max(cnt, 1));
+      double rad = 0;
+      for (int l = 0; l < SD_TILE; ++l) {
+        const int j = lslots[t * SD_TILE + l];
+        if (j < 0) continue;
+        double s2 = 0;
+        for (int k = 0; k < 3; ++k) {
+          const double dd = d.lig_xyz[(size_t)j * 3 + k] - (double)cf[k];
+          s2 += dd * dd;
+        }
+        rad = std::max(rad, std::sqrt(s2));
+      }
+      lch[t] = make_float4(cf[0], cf[1], cf[2], round_up_f(rad * (1 + 1e-6) + 1e-4));
+    }
+    int rc2;
+    if ((rc2 = upload(c, h, lslots.data(), lslots.size(), &D.l_perm))) return rc2;
+    if ((rc2 = upload(c, h, lch.data(), lch.size(), &D.l_chunk))) return rc2;
+  }
   std::vector<int> lcol(d.n_lig), llj(d.n_lig, 0);
   std::vector<float> lq(d.n_lig, 0.f);
   for (int j = 0; j < d.n_lig; ++j) {
@@ -382,12 +416,14 @@ int rebuild_worklist(sd_ctx* c) {
 int configure_score(sd_ctx* c, int precision, int* grid, size_t* smem) {
   const size_t sm = score_smem_bytes(precision, c->scoring, c->max_nr, c->max_nl);
   const void* k = score_kernel_ptr(precision, c->scoring);
+  const int threads = score_threads_of(precision, c->scoring);
   SD_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(sm, 1)));
   int per_sm = 0;
-  SD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, c->score_threads, sm));
+  SD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, sm));
   if (per_sm < 1) return fail(SD_ERR_ARG, "scoring kernel does not fit on an SM (shared memory)");
   *grid = per_sm * c->nsm;
   *smem = sm;
+  c->score_threads = threads;
   return SD_OK;
 }
 
@@ -822,14 +858,64 @@ int sd_dfire_bins(sd_ctx* c, int ci, const double* pose, int precision, int* bin
 
 int sd_pydock_grad(sd_ctx* c, int ci, const double* poses, int n, int precision, double* energy_out,
                    double* grad_out) {
-  (void)c;
-  (void)ci;
-  (void)poses;
-  (void)n;
-  (void)precision;
-  (void)energy_out;
-  (void)grad_out;
-  return fail(SD_ERR_NOTSUP, "sd_pydock_grad: not built yet");
+  if (!c || !poses || !grad_out || n < 0 || ci < 0 || ci >= c->ncplx)
+    return fail(SD_ERR_ARG, "sd_pydock_grad: bad arguments");
+  if (c->scoring != SD_SCORING_PYDOCK) return fail(SD_ERR_ARG, "sd_pydock_grad: context scoring is not pyDock");
+  if (precision < SD_PREC_FP64_REF || precision > SD_PREC_MIXED)
+    return fail(SD_ERR_ARG, "sd_pydock_grad: unknown precision");
+  if (n == 0) return SD_OK;
+  if (n >= (1 << 24)) return fail(SD_ERR_ARG, "sd_pydock_grad: more than 2^24 poses");
+  SD_CUDA(cudaSetDevice(c->device));
+  const DevComplex& D = c->cx[ci].d;
+  const int ng = 6 + D.nmr + D.nml;
+  for (size_t i = 0; i < (size_t)n * D.pl; ++i)
+    if (!std::isfinite(poses[i])) return fail(SD_ERR_NUMERIC, "sd_pydock_grad: non-finite pose");
+  int rc;
+  if ((rc = ensure(c, c->s_pose, (size_t)n * D.pl * 8))) return rc;
+  if ((rc = ensure(c, c->s_score, (size_t)n * 8))) return rc;
+  if ((rc = ensure(c, c->s_energy, (size_t)n * 8))) return rc;
+  if ((rc = ensure(c, c->s_ref, (size_t)n * 3 * 8))) return rc;
+  if ((rc = ensure(c, c->s_work, (size_t)n * 4))) return rc;
+  if ((rc = ensure(c, c->s_grad, (size_t)n * ng * 8))) return rc;
+  std::vector<int> work(n);
+  for (int i = 0; i < n; ++i) work[i] = wi_pack(ci, i);
+  DevComplex S = D;
+  S.pos = (double*)c->s_pose.p;
+  S.scoring = (double*)c->s_score.p;
+  S.ref = (double*)c->s_ref.p;
+  StepCtl ctl;
+  SD_CUDA(cudaMemcpy(&ctl, c->d_ctl_scratch, sizeof ctl, cudaMemcpyDeviceToHost));
+  ctl.count[0] = n;
+  ctl.count[1] = 0;
+  ctl.grab[0] = ctl.grab[1] = 0;
+  ctl.parity = 0;
+  SD_CUDA(cudaMemcpyAsync(c->s_pose.p, poses, (size_t)n * D.pl * 8, cudaMemcpyHostToDevice, c->stream));
+  SD_CUDA(cudaMemcpyAsync(c->s_work.p, work.data(), (size_t)n * 4, cudaMemcpyHostToDevice, c->stream));
+  SD_CUDA(cudaMemcpyAsync(&c->d_cplx_scratch[ci], &S, sizeof S, cudaMemcpyHostToDevice, c->stream));
+  SD_CUDA(cudaMemcpyAsync(c->d_ctl_scratch, &ctl, sizeof ctl, cudaMemcpyHostToDevice, c->stream));
+  const size_t sm = pydock_smem_bytes(precision, true, c->max_nl, c->max_nr);
+  const void* k = pydock_kernel_ptr(precision, true);
+  SD_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  int per_sm = 0;
+  SD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, pydock_threads(), sm));
+  if (per_sm < 1) return fail(SD_ERR_ARG, "pyDock gradient kernel does not fit on an SM (shared memory)");
+  ScoreLaunch L{};
+  L.cplx = c->d_cplx_scratch;
+  L.ctl = c->d_ctl_scratch;
+  L.work[0] = (const int*)c->s_work.p;
+  L.work[1] = (const int*)c->s_work.p;
+  L.table64 = c->d_table64;
+  L.table32 = c->d_table32;
+  L.lj_eps = c->d_lj_eps;
+  L.lj_sigma = c->d_lj_sigma;
+  L.energy_out = (double*)c->s_energy.p;
+  if ((rc = pydock_launch(L, precision, true, (double*)c->s_grad.p, per_sm * c->nsm, sm, c->stream)))
+    return fail(rc, std::string("pyDock gradient kernel: ") + cudaGetErrorString(cudaGetLastError()));
+  if (energy_out)
+    SD_CUDA(cudaMemcpyAsync(energy_out, c->s_energy.p, (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));
+  SD_CUDA(cudaMemcpyAsync(grad_out, c->s_grad.p, (size_t)n * ng * 8, cudaMemcpyDeviceToHost, c->stream));
+  SD_CUDA(cudaStreamSynchronize(c->stream));
+  return SD_OK;
 }
 
 }  // extern "C"

@@ -52,6 +52,10 @@ struct DevComplex {
   const int* l_col;        // [nl] tL*20
   const float* l_q;
   const int* l_lj;
+  // ligand in spatial chunks of 32 (mixed precision only; order-free sums)
+  int nlchunks;
+  const int* l_perm;       // [nlchunks*32] chunk slot -> original ligand index, or -1
+  const float4* l_chunk;   // [nlchunks] centre (ligand frame) + radius
   float mnorm_r[SD_MAX_MODES], mnorm_l[SD_MAX_MODES];  // max per-atom mode norm (rounded up)
   float lig_radius;        // max |l0_j| (rounded up)
   float rec_span;          // max |r0_i - origin| (rounded up)
@@ -118,14 +122,16 @@ struct GsoLaunch {
 int score_launch(const ScoreLaunch& L, int precision, int scoring, int grid, int threads, size_t smem,
                  cudaStream_t st);
 size_t score_smem_bytes(int precision, int scoring, int max_nr, int max_nl);
+int score_threads_of(int precision, int scoring);
 const void* score_kernel_ptr(int precision, int scoring);
 int gso_launch(const GsoLaunch& L, int threads, cudaStream_t st);
 int bins_launch(const DevComplex* cplx, int c, const double* d_pose, int precision, int* d_bins, int nr, int nl,
                 int* d_fallback, cudaStream_t st);
-int pydock_grad_launch(const ScoreLaunch& L, int precision, int n, double* d_energy, double* d_grad, int grid,
-                       int threads, size_t smem, cudaStream_t st);
-size_t pydock_grad_smem_bytes(int max_nl);
-const void* pydock_grad_kernel_ptr(int precision);
+size_t pydock_smem_bytes(int precision, bool grad, int max_nl, int max_nr);
+const void* pydock_kernel_ptr(int precision, bool grad);
+int pydock_launch(const ScoreLaunch& L, int precision, bool grad, double* out_grad, int grid, size_t smem,
+                  cudaStream_t st);
+int pydock_threads();
 void set_key_thresholds(const double* t64);
 
 }  // namespace sd

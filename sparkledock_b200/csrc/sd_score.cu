@@ -89,12 +89,13 @@ __global__ void __launch_bounds__(256) dfire_score_kernel(ScoreLaunch L) {
   __shared__ int sh_lut[32];
   __shared__ double sh_red[32];
   __shared__ int sh_item;
+  __shared__ int sh_ntile, sh_next;
   __shared__ float sh_bound[4];  // dR, dL, B (mixed), unused
   __shared__ unsigned long long sh_fallback, sh_z, sh_cut, sh_pairs, sh_evals;
 
   constexpr bool kCull = PREC != SD_PREC_FP64_REF;
   constexpr bool kMixed = PREC == SD_PREC_MIXED;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid < 32) {
     sh_T[tid] = c_T[tid];
     sh_Tf[tid] = c_Tf[tid];
@@ -151,6 +152,11 @@ __global__ void __launch_bounds__(256) dfire_score_kernel(ScoreLaunch L) {
     float4* ligF = reinterpret_cast<float4*>(smem);  // centred FP32 (x,y,z, col bits)
     LigD* ligD = reinterpret_cast<LigD*>(smem + (size_t)16 * ((nl + 1) & ~1));
     double* vacc = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(ligD) + (size_t)32 * nl);
+    int* tlist = reinterpret_cast<int*>(vacc + nr);  // tiles within reach of the ligand
+    if (tid == 0) {
+      sh_ntile = 0;
+      sh_next = 0;
+    }
     for (int j = tid; j < nl; j += blockDim.x) {
       double x, y, z;
       ligand_exact(C, j, sh_pose, sh_q, sh_qi, x, y, z);
@@ -173,18 +179,32 @@ __global__ void __launch_bounds__(256) dfire_score_kernel(ScoreLaunch L) {
     const float dR = sh_bound[0], dL = sh_bound[1], B = sh_bound[2];
     const float tile_reach_base = 15.0f + dR + SD_CULL_MARGIN;
     const float lig_reach = C.lig_radius + dL;
+    for (int k = tid; k < C.ntiles; k += blockDim.x) {
+      bool keep = true;
+      if (kCull) {
+        const float4 tile = C.r_tile[k];
+        const float cx = (float)((double)tile.x - tx), cy = (float)((double)tile.y - ty),
+                    cz = (float)((double)tile.z - tz);
+        const float reach = tile_reach_base + tile.w + lig_reach;
+        keep = cx * cx + cy * cy + cz * cz <= reach * reach;
+      }
+      if (keep) tlist[atomicAdd(&sh_ntile, 1)] = k;
+    }
+    __syncthreads();
+    const int ntile = sh_ntile;
     float ks = 0.f, kc = 0.f;  // MIXED per-thread Kahan state across tiles
     unsigned long long nfb = 0;
 
-    for (int k = warp; k < C.ntiles; k += nwarps) {
+    for (;;) {
+      int ti = 0;
+      if (lane == 0) ti = atomicAdd(&sh_next, 1);
+      ti = __shfl_sync(0xffffffffu, ti, 0);
+      if (ti >= ntile) break;
+      const int k = tlist[ti];
       const float4 tile = C.r_tile[k];
       const float cx = (float)((double)tile.x - tx), cy = (float)((double)tile.y - ty),
                   cz = (float)((double)tile.z - tz);
       const float reach = tile_reach_base + tile.w;
-      if (kCull) {
-        const float dd = sqrtf(cx * cx + cy * cy + cz * cz);
-        if (dd > reach + lig_reach) continue;  // whole tile out of range of the whole ligand
-      }
       const float reach2 = reach * reach;
       const int slot = k * SD_TILE + lane;
       const int orig = C.r_orig[slot];
@@ -310,29 +330,44 @@ __global__ void __launch_bounds__(256) dfire_score_kernel(ScoreLaunch L) {
   }
 }
 
+}  // namespace sd
+
+#include "sd_score_mixed.cuh"
+
+namespace sd {
+
 size_t score_smem_bytes(int precision, int scoring, int max_nr, int max_nl) {
-  (void)scoring;
-  size_t b = (size_t)16 * ((max_nl + 1) & ~1);
-  if (precision != SD_PREC_MIXED) b += (size_t)32 * max_nl + (size_t)8 * max_nr;
-  return b;
+  if (scoring == SD_SCORING_PYDOCK) return pydock_smem_bytes(precision, false, max_nl, max_nr);
+  if (precision == SD_PREC_MIXED) {
+    const size_t nlc = (size_t)(max_nl + SD_TILE - 1) / SD_TILE;
+    const size_t ntiles = (size_t)(max_nr + SD_TILE - 1) / SD_TILE;
+    return (size_t)16 * (nlc * SD_TILE + nlc) + 4 * ntiles;
+  }
+  return (size_t)16 * ((max_nl + 1) & ~1) + (size_t)32 * max_nl + (size_t)8 * max_nr +
+         (size_t)4 * ((max_nr + SD_TILE - 1) / SD_TILE);
+}
+
+int score_threads_of(int precision, int scoring) {
+  if (scoring == SD_SCORING_PYDOCK) return pydock_threads();
+  return precision == SD_PREC_MIXED ? kWarps * 32 : 256;
 }
 
 const void* score_kernel_ptr(int precision, int scoring) {
-  (void)scoring;
+  if (scoring == SD_SCORING_PYDOCK) return pydock_kernel_ptr(precision, false);
   switch (precision) {
     case SD_PREC_FP64_REF: return (const void*)dfire_score_kernel<SD_PREC_FP64_REF>;
     case SD_PREC_FP64: return (const void*)dfire_score_kernel<SD_PREC_FP64>;
-    default: return (const void*)dfire_score_kernel<SD_PREC_MIXED>;
+    default: return (const void*)dfire_score_mixed_kernel;
   }
 }
 
 int score_launch(const ScoreLaunch& L, int precision, int scoring, int grid, int threads, size_t smem,
                  cudaStream_t st) {
-  (void)scoring;
+  if (scoring == SD_SCORING_PYDOCK) return pydock_launch(L, precision, false, nullptr, grid, smem, st);
   switch (precision) {
     case SD_PREC_FP64_REF: dfire_score_kernel<SD_PREC_FP64_REF><<<grid, threads, smem, st>>>(L); break;
     case SD_PREC_FP64: dfire_score_kernel<SD_PREC_FP64><<<grid, threads, smem, st>>>(L); break;
-    default: dfire_score_kernel<SD_PREC_MIXED><<<grid, threads, smem, st>>>(L); break;
+    default: dfire_score_mixed_kernel<<<grid, threads, smem, st>>>(L); break;
   }
   return cudaGetLastError() == cudaSuccess ? SD_OK : SD_ERR_CUDA;
 }

@@ -64,3 +64,25 @@ def test_ctx_create_without_gpu_is_a_status_not_a_crash(tables):
         assert e.code == _abi.SD_ERR_CUDA
     else:
         raise AssertionError("expected SD_ERR_CUDA without a device")
+
+
+def test_gso_output_writer_format(tmp_path):
+    """gso_<steps>.out matches the reference writer's line format (prepare_gso_task.cu:2850-2904)."""
+    import ctypes as C
+    S, G, pl = 2, 3, 27
+    rng = np.random.default_rng(0)
+    pos = rng.normal(size=(S, G, pl))
+    luc = rng.normal(size=(S, G))
+    nn = rng.integers(0, 6, size=(S, G)).astype(np.int32)
+    vr = rng.uniform(0, 5, size=(S, G))
+    sc = rng.normal(size=(S, G))
+    rc = _abi.lib().sd_write_gso_output(str(tmp_path).encode(), 7, S, G, pl, 100, _abi.dptr(pos), _abi.dptr(luc),
+                                        _abi.iptr(nn), _abi.dptr(vr), _abi.dptr(sc))
+    assert rc == 0
+    for s in range(S):
+        lines = open(tmp_path / f"swarm_{7 + s}" / "gso_100.out").read().split("\n")
+        assert lines[0] == "#Coordinates  RecID  LigID  Luciferin  Neighbor's number  Vision Range  Scoring"
+        for g in range(G):
+            exp = "(" + ", ".join("%f" % v for v in pos[s, g]) + ")\t0\t0\t" + "%f" % luc[s, g] + "\t" + \
+                  str(nn[s, g]) + "\t" + "%f" % vr[s, g] + "\t" + "%f" % sc[s, g] + "\t"
+            assert lines[1 + g] == exp

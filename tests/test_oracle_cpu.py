@@ -211,3 +211,16 @@ def test_golden_vectors():
         oracle_step(osys, st, U[:, t, :])
     for f in ("pos", "luciferin", "vision", "select", "nnei", "scoring"):
         assert np.array_equal(getattr(st, f), z["final_" + f]), f
+
+
+def test_pydock_oracle_gradient_matches_finite_differences(tables):
+    """The FP64 oracle gradient of the pyDock-style energy equals central differences (h=1e-4)."""
+    from pydock_util import fd_grad, oracle_grad
+    cx = sd.SyntheticComplex(300, 200, 1, 6, seed=31)
+    osys = OracleSystem(cx, tables, scoring=1)
+    ng = 6 + cx.n_modes_rec + cx.n_modes_lig
+    for pose in cx.poses.reshape(-1, cx.pose_len)[:3]:
+        g = oracle_grad(osys, pose, ng)
+        f = fd_grad(osys, pose, ng)
+        scale = max(np.abs(g).max(), 1.0)
+        assert np.abs(g - f).max() / scale < 1e-6, (g, f)
