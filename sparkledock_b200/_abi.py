@@ -61,7 +61,7 @@ class SwarmState(C.Structure):
 class Stats(C.Structure):
     _fields_ = [(n, C.c_longlong) for n in (
         "scored_poses", "steps", "pairs_fallback", "edge_d2_zero", "edge_d2_cutoff",
-        "edge_u_zero", "edge_shortfall", "timeouts", "pairs_in_cutoff", "pairs_evaluated")]
+        "edge_u_zero", "edge_shortfall", "timeouts", "pairs_in_cutoff", "pairs_evaluated", "guard_errors")]
 
 
 class SynthSpec(C.Structure):

@@ -771,6 +771,7 @@ int sd_get_stats(sd_ctx* c, sd_stats* out) {
   out->timeouts = (long long)(a.stats[ST_TIMEOUT] + b.stats[ST_TIMEOUT]);
   out->pairs_in_cutoff = (long long)a.stats[ST_PAIRS];
   out->pairs_evaluated = (long long)a.stats[ST_EVALS];
+  out->guard_errors = (long long)(a.stats[ST_GUARD] + b.stats[ST_GUARD]);
   return SD_OK;
 }
 

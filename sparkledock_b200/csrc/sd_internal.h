@@ -85,7 +85,7 @@ struct StepCtl {
   unsigned long long stats[12];  // mirrors sd_stats order
 };
 
-enum { ST_SCORED = 0, ST_STEPS, ST_FALLBACK, ST_D2ZERO, ST_D2CUT, ST_UZERO, ST_SHORT, ST_TIMEOUT, ST_PAIRS, ST_EVALS };
+enum { ST_SCORED = 0, ST_STEPS, ST_FALLBACK, ST_D2ZERO, ST_D2CUT, ST_UZERO, ST_SHORT, ST_TIMEOUT, ST_PAIRS, ST_EVALS, ST_GUARD };
 
 struct GsoParamsDev {
   double rho, gamma, beta, max_vision, step_t, step_r, step_nm;

@@ -1,30 +1,35 @@
 // Mixed-precision DFIRE scoring (FP32 distances, exact bins, compensated FP32 sums).
+// Included by sd_score.cu (shares its constant-memory key thresholds and bin table).
 //
 // Same contract as the FP64 kernels in sd_score.cu (energy of cdfire_calculate_dfire,
 // prepare_gso_tasks.cc:1522-1615, with every bin identical to the FP64 reference bin), but the
-// summation order is free, which this kernel uses three ways:
-//  * the ligand is kept in spatial chunks of 32 atoms (k-d order, ligand frame), so a receptor
-//    tile first rejects whole ligand chunks by bounding spheres, then single atoms by ballot;
-//  * stage 1 (one lane per receptor atom, one ligand atom broadcast per iteration) only tests
-//    d^2 and appends the in-cutoff pairs {d^2, table row+column, pair id} to a per-warp ring
-//    in shared memory (warp-aggregated compaction);
-//  * stage 2 drains the ring 64 pairs at a time, two independent pairs per lane: key from a
-//    fast reciprocal square root, the exact-bin guard against the proven FP32 error bound B,
-//    two table gathers in flight, Kahan accumulation.  Pairs within B of a bin edge or of the
-//    cutoff are recomputed from the exact FP64 pose transform (counted as fallbacks).
-// Included by sd_score.cu (shares its constant-memory key thresholds and bin table).
+// summation order is free, which this kernel uses:
+//  * the ligand is kept in spatial chunks of 32 atoms (k-d order, ligand frame); a receptor
+//    tile (one warp, one lane per receptor atom) rejects whole ligand chunks by bounding
+//    spheres, then single atoms by ballot, and collects the surviving ligand atoms as
+//    candidates;
+//  * stage 1 takes candidates 32 at a time: their coordinates are staged once in a per-warp
+//    buffer, every lane tests its receptor atom against all 32 (fully unrolled, broadcast
+//    reads) and keeps a 32-bit in-cutoff mask; one warp scan per batch then appends the
+//    in-cutoff pairs (ligand slot, lane) to a per-warp ring;
+//  * stage 2 drains the ring 64 pairs at a time, two per lane: recompute d^2 (same FP32
+//    expression, so the same value), key from a fast reciprocal square root, the exact-bin
+//    guard against the proven FP32 error bound B, two table gathers in flight, Kahan sums.
+//    Pairs within B of a bin edge or of the cutoff are recomputed from the exact FP64 pose
+//    transform (counted as fallbacks).
 #pragma once
 
 namespace sd {
 namespace {
 
 constexpr int kWarps = 4;
-constexpr int kRing = 128;  // entries per warp ring (power of two)
+constexpr int kRing = 1024;  // per-warp ring of in-cutoff pairs (a batch adds at most 32*32)
 
-struct Ring {
-  float d2[kWarps][kRing];
-  int base[kWarps][kRing];
-  int pid[kWarps][kRing];
+struct __align__(16) WarpBufs {
+  float4 cand_xyz[32];   // staged candidate ligand atoms (centred FP32, col bits)
+  int cand_slot[64];     // pending candidate ligand slots
+  float4 rec[32];        // this tile's receptor atoms (centred FP32, row bits)
+  int ring[kRing];       // packed (ligand slot << 5 | lane)
 };
 
 __device__ __forceinline__ int exact_key_m(double d2, const double* T) {
@@ -43,25 +48,25 @@ struct PoseCtx {
   const double* q;
   const double* qi;
   const double* T;
-  const float* Tf;
-  const int* lut;
+  const float4* key4;  // per key: {lower threshold, upper threshold, bin bits, 0}
   const float* table;
   float B;
 };
 
-// value of one in-cutoff candidate pair; returns false when the exact FP64 distance shows the
-// pair is outside the cutoff
-__device__ __forceinline__ bool pair_value(const PoseCtx& P, float d2, int base, int pid, float& val,
+// value of one in-cutoff candidate pair (slot = receptor slot, ls = ligand chunk slot);
+// returns false when the exact FP64 distance shows the pair is outside the cutoff
+__device__ __forceinline__ bool pair_value(const PoseCtx& P, float d2, int base, int slot, int ls, float& val,
                                            unsigned long long& nfb, unsigned long long& nz, unsigned long long& ncut) {
   // key estimate; d2 == 0 gives NaN -> 0 and is caught by the edge guard below
   const float r = d2 * rsqrtf(d2);
   int key = (int)fmaf(r, 2.0f, -1.0f);
   key = key < 0 ? 0 : (key > 29 ? 29 : key);
-  const bool near = (d2 - P.Tf[key] <= P.B) || (P.Tf[key + 1] - d2 <= P.B);
+  const float4 kk = P.key4[key];
+  int bin = __float_as_int(kk.z);
+  const bool near = (d2 - kk.x <= P.B) || (kk.y - d2 <= P.B);
   if (near) {
     ++nfb;
-    const int slot = pid >> 13, lslot = pid & 8191;
-    const int j = P.C->l_perm[lslot];
+    const int j = P.C->l_perm[ls];
     double rx, ry, rz, lx, ly, lz;
     receptor_exact(*P.C, P.nslots, slot, P.pose, rx, ry, rz);
     ligand_exact(*P.C, j, P.pose, P.q, P.qi, lx, ly, lz);
@@ -75,21 +80,21 @@ __device__ __forceinline__ bool pair_value(const PoseCtx& P, float d2, int base,
       key = exact_key_m(e2, P.T);
       if (key == 29) ++ncut;
     }
+    bin = __float_as_int(P.key4[key].z);
   }
-  val = P.table[base + P.lut[key]];
+  val = P.table[base + bin];
   return true;
 }
 
 }  // namespace
 
-__global__ void __launch_bounds__(kWarps * 32, 5) dfire_score_mixed_kernel(ScoreLaunch L) {
+__global__ void __launch_bounds__(kWarps * 32, 4) dfire_score_mixed_kernel(ScoreLaunch L) {
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ Ring ring;
+  __shared__ WarpBufs wb[kWarps];
   __shared__ double sh_pose[7 + 2 * SD_MAX_MODES];
   __shared__ double sh_q[4], sh_qi[4];
   __shared__ double sh_T[32];
-  __shared__ float sh_Tf[32];
-  __shared__ int sh_lut[32];
+  __shared__ float4 sh_key4[32];
   __shared__ double sh_red[32];
   __shared__ int sh_item;
   __shared__ int sh_ntile, sh_next;
@@ -100,16 +105,17 @@ __global__ void __launch_bounds__(kWarps * 32, 5) dfire_score_mixed_kernel(Score
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid < 32) {
     sh_T[tid] = c_T[tid];
-    sh_Tf[tid] = c_Tf[tid];
-    sh_lut[tid] = c_binlut[tid];
+    const int k = tid < 30 ? tid : 29;
+    sh_key4[tid] = make_float4(c_Tf[k], c_Tf[k + 1], __int_as_float(c_binlut[k]), 0.f);
   }
   if (tid == 0) sh_fallback = sh_z = sh_cut = sh_pairs = sh_evals = 0;
   StepCtl* ctl = L.ctl;
   const int parity = ctl->parity;
   const int count = ctl->count[parity];
   const int* work = L.work[parity];
-  unsigned long long n_done = 0, nfb = 0, nz = 0, ncut = 0, npairs = 0, nevals = 0;
+  unsigned long long n_done = 0, nfb = 0, nz = 0, ncut = 0, npairs = 0, nevals = 0, nguard = 0;
   const unsigned lt_mask = (1u << lane) - 1u;
+  WarpBufs& W = wb[warp];
 
   for (;;) {
     __syncthreads();
@@ -120,7 +126,7 @@ __global__ void __launch_bounds__(kWarps * 32, 5) dfire_score_mixed_kernel(Score
     const int w = work[item];
     const int ci = wi_complex(w), p = wi_local(w);
     const DevComplex& C = L.cplx[ci];
-    const int nslots = nslots_of(C), pl = C.pl, nlc = C.nlchunks;
+    const int nslots = nslots_of(C), pl = C.pl, nlc = C.nlchunks, nls = nlc * SD_TILE;
     const double* pose_g = C.pos + (size_t)p * pl;
     if (tid < pl) sh_pose[tid] = pose_g[tid];
     __syncthreads();
@@ -134,10 +140,11 @@ __global__ void __launch_bounds__(kWarps * 32, 5) dfire_score_mixed_kernel(Score
       dL = dL * 1.0001f + 1e-4f;
       sh_bound[0] = dR;
       sh_bound[1] = dL;
+      // bound of |FP32 d2 - FP64 d2| for pairs within 15.1 A (coordinates centred on t)
       const float RL = C.lig_radius + dL;
       const float u32 = 5.9604645e-8f;
       sh_bound[2] = 2.0f * (2.02f * u32 * (26.2f * (2.0f * RL + 15.1f) + 228.0f) + 3.0f * u32 * 228.0f) + 1e-6f;
-      // rotation matrix of the unit quaternion (chunk centres only; culling margin covers it)
+      // rotation matrix of the unit quaternion (chunk centres only; the culling margin covers it)
       const double n = sqrt(sh_q[0] * sh_q[0] + sh_q[1] * sh_q[1] + sh_q[2] * sh_q[2] + sh_q[3] * sh_q[3]);
       const float w0 = (float)(sh_q[0] / n), x = (float)(sh_q[1] / n), y = (float)(sh_q[2] / n),
                   z = (float)(sh_q[3] / n);
@@ -150,23 +157,22 @@ __global__ void __launch_bounds__(kWarps * 32, 5) dfire_score_mixed_kernel(Score
       sh_rot[6] = 2 * (x * z - w0 * y);
       sh_rot[7] = 2 * (y * z + w0 * x);
       sh_rot[8] = 1 - 2 * (x * x + y * y);
+      // ligand reference point (prepare_gso_tasks.cc:460, :513, :524-526)
       double rx = C.lig_ref[0], ry = C.lig_ref[1], rz = C.lig_ref[2];
       quat_rotate(sh_q, sh_qi, rx, ry, rz);
       double* ref = C.ref + (size_t)p * 3;
       ref[0] = rx + sh_pose[0];
       ref[1] = ry + sh_pose[1];
       ref[2] = rz + sh_pose[2];
+      sh_ntile = 0;
+      sh_next = 0;
     }
     __syncthreads();
     const double tx = sh_pose[0], ty = sh_pose[1], tz = sh_pose[2];
     const float dR = sh_bound[0], dL = sh_bound[1];
-    float4* ligS = reinterpret_cast<float4*>(smem);               // [nlc*32] centred, col bits
-    float4* chS = ligS + (size_t)nlc * SD_TILE;                   // [nlc] centre + radius
-    int* tlist = reinterpret_cast<int*>(chS + nlc);               // [ntiles] tiles within reach
-    if (tid == 0) {
-      sh_ntile = 0;
-      sh_next = 0;
-    }
+    float4* ligS = reinterpret_cast<float4*>(smem);  // [nlc*32] centred, col bits
+    float4* chS = ligS + (size_t)nlc * SD_TILE;      // [nlc] centre + radius
+    int* tlist = reinterpret_cast<int*>(chS + nlc);  // [ntiles] tiles within reach
     for (int s = tid; s < nlc * SD_TILE; s += blockDim.x) {
       const int j = C.l_perm[s];
       if (j >= 0) {
@@ -184,9 +190,7 @@ __global__ void __launch_bounds__(kWarps * 32, 5) dfire_score_mixed_kernel(Score
       const float Z = sh_rot[6] * cc.x + sh_rot[7] * cc.y + sh_rot[8] * cc.z;
       chS[c] = make_float4(X, Y, Z, cc.w + dL);
     }
-    __syncthreads();
     const float lig_reach = C.lig_radius + dL;
-    // tiles whose sphere can reach the ligand sphere (order is free: sums are order-free here)
     for (int k = tid; k < C.ntiles; k += blockDim.x) {
       const float4 tile = C.r_tile[k];
       const float cx = (float)((double)tile.x - tx), cy = (float)((double)tile.y - ty),
@@ -196,38 +200,9 @@ __global__ void __launch_bounds__(kWarps * 32, 5) dfire_score_mixed_kernel(Score
     }
     __syncthreads();
     const int ntile = sh_ntile;
-    PoseCtx P{&C, nslots, sh_pose, sh_q, sh_qi, sh_T, sh_Tf, sh_lut, L.table32, sh_bound[2]};
+    PoseCtx P{&C, nslots, sh_pose, sh_q, sh_qi, sh_T, sh_key4, L.table32, sh_bound[2]};
+    const float cut2 = 225.0f + P.B;
     float ks = 0.f, kc = 0.f;
-    int head = 0, tail = 0;  // warp-uniform ring cursors
-    float* rd2 = ring.d2[warp];
-    int* rbase = ring.base[warp];
-    int* rpid = ring.pid[warp];
-
-    auto kahan = [&](float v) {
-      const float y = v - kc;
-      const float t = ks + y;
-      kc = (t - ks) - y;
-      ks = t;
-    };
-    // stage 2: consume n (<= 64) ring entries, two per lane
-    auto drain = [&](int n) {
-      const int i0 = tail + lane, i1 = tail + 32 + lane;
-      const bool v0 = lane < n, v1 = lane + 32 < n;
-      float a0 = 0.f, a1 = 0.f;
-      bool k0 = false, k1 = false;
-      if (v0) k0 = pair_value(P, rd2[i0 & (kRing - 1)], rbase[i0 & (kRing - 1)], rpid[i0 & (kRing - 1)], a0, nfb, nz, ncut);
-      if (v1) k1 = pair_value(P, rd2[i1 & (kRing - 1)], rbase[i1 & (kRing - 1)], rpid[i1 & (kRing - 1)], a1, nfb, nz, ncut);
-      if (k0) {
-        kahan(a0);
-        ++npairs;
-      }
-      if (k1) {
-        kahan(a1);
-        ++npairs;
-      }
-      tail += n;
-      __syncwarp();
-    };
 
     for (;;) {
       int ti = 0;
@@ -241,8 +216,7 @@ __global__ void __launch_bounds__(kWarps * 32, 5) dfire_score_mixed_kernel(Score
       const float reach = 15.0f + dR + SD_CULL_MARGIN + tile.w;
       const float reach2 = reach * reach;
       const int slot = k * SD_TILE + lane;
-      const int orig = C.r_orig[slot];
-      const bool active = orig >= 0;
+      const bool active = C.r_orig[slot] >= 0;
       float fx = 1e18f, fy = 1e18f, fz = 1e18f;
       int row = 0;
       if (active) {
@@ -253,7 +227,105 @@ __global__ void __launch_bounds__(kWarps * 32, 5) dfire_score_mixed_kernel(Score
         fz = (float)(rz - tz);
         row = C.r_row[slot];
       }
-      const float cut2 = 225.0f + P.B;
+      W.rec[lane] = make_float4(fx, fy, fz, __int_as_float(row));
+      const int nact = __popc(__ballot_sync(0xffffffffu, active));
+      int ncand = 0, head = 0, tail = 0;  // warp-uniform
+
+      // stage 2: consume n (<= 64) ring entries, two per lane
+      auto drain = [&](int n) {
+        const int i0 = tail + lane, i1 = tail + 32 + lane;
+        const bool v0 = lane < n, v1 = lane + 32 < n;
+        float a0 = 0.f, a1 = 0.f;
+        bool k0 = false, k1 = false;
+        if (v0) {
+          const int e = W.ring[i0 & (kRing - 1)];
+          const int ls = e >> 5, rl = e & 31;
+          if ((unsigned)ls >= (unsigned)nls) {  // guard: never taken unless the ring is corrupt
+            ++nguard;
+          } else {
+          const float4 R = W.rec[rl], Lg = ligS[ls];
+          const float ex = R.x - Lg.x, ey = R.y - Lg.y, ez = R.z - Lg.z;
+          const float d2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
+          k0 = pair_value(P, d2, __float_as_int(R.w) + __float_as_int(Lg.w), k * SD_TILE + rl, ls, a0, nfb, nz, ncut);
+          }
+        }
+        if (v1) {
+          const int e = W.ring[i1 & (kRing - 1)];
+          const int ls = e >> 5, rl = e & 31;
+          if ((unsigned)ls >= (unsigned)nls) {  // guard: never taken unless the ring is corrupt
+            ++nguard;
+          } else {
+          const float4 R = W.rec[rl], Lg = ligS[ls];
+          const float ex = R.x - Lg.x, ey = R.y - Lg.y, ez = R.z - Lg.z;
+          const float d2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
+          k1 = pair_value(P, d2, __float_as_int(R.w) + __float_as_int(Lg.w), k * SD_TILE + rl, ls, a1, nfb, nz, ncut);
+          }
+        }
+        if (k0) {
+          const float y = a0 - kc;
+          const float t = ks + y;
+          kc = (t - ks) - y;
+          ks = t;
+          ++npairs;
+        }
+        if (k1) {
+          const float y = a1 - kc;
+          const float t = ks + y;
+          kc = (t - ks) - y;
+          ks = t;
+          ++npairs;
+        }
+        tail += n;
+      };
+      // stage 1: test the first 32 pending candidates against every lane's receptor atom
+      auto batch = [&](int nb) {
+        __syncwarp();
+        // unused candidate places sit at -1e18, inactive receptor lanes at +1e18: never in range
+        if (lane < nb) W.cand_xyz[lane] = ligS[W.cand_slot[lane]];
+        else W.cand_xyz[lane] = make_float4(-1e18f, -1e18f, -1e18f, 0.f);
+        __syncwarp();
+        unsigned m = 0;
+#pragma unroll
+        for (int b = 0; b < 32; ++b) {
+          const float4 l = W.cand_xyz[b];
+          const float ex = fx - l.x, ey = fy - l.y, ez = fz - l.z;
+          const float d2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
+          m |= (d2 <= cut2 ? 1u : 0u) << b;
+        }
+        // only real candidates and real receptor atoms may produce pairs
+        m &= active ? (nb >= 32 ? 0xffffffffu : ((1u << nb) - 1u)) : 0u;
+        nevals += (unsigned long long)(lane == 0 ? nb * nact : 0);
+        // exclusive scan of the per-lane pair counts
+        const int cnt = __popc(m);
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += v;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        if (head - tail + total > kRing)  // only for very dense batches: empty the ring first
+          while (head - tail > 0) drain(min(64, head - tail));
+        int pos = head + incl - cnt;
+        while (m) {
+          const int b = __ffs(m) - 1;
+          m &= m - 1;
+          W.ring[pos & (kRing - 1)] = (W.cand_slot[b] << 5) | lane;
+          ++pos;
+        }
+        head += total;
+        __syncwarp();
+        // keep the candidates beyond the first 32
+        const int rest = ncand - nb;
+        int carry = 0;
+        if (lane < rest) carry = W.cand_slot[32 + lane];
+        __syncwarp();
+        if (lane < rest) W.cand_slot[lane] = carry;
+        ncand = rest;
+        __syncwarp();
+        while (head - tail >= 64) drain(64);
+      };
+
       for (int cb = 0; cb < nlc; cb += 32) {
         const int c = cb + lane;
         bool cnear = false;
@@ -266,34 +338,20 @@ __global__ void __launch_bounds__(kWarps * 32, 5) dfire_score_mixed_kernel(Score
         while (cm) {
           const int cc = cb + __ffs(cm) - 1;
           cm &= cm - 1;
-          const int sbase = cc * SD_TILE;
-          const float4 la = ligS[sbase + lane];
+          const int sb = cc * SD_TILE;
+          const float4 la = ligS[sb + lane];
           const float ax = la.x - cx, ay = la.y - cy, az = la.z - cz;
-          unsigned am = __ballot_sync(0xffffffffu, ax * ax + ay * ay + az * az <= reach2);
-          while (am) {
-            const int b = __ffs(am) - 1;
-            am &= am - 1;
-            const int ls = sbase + b;
-            const float4 l = ligS[ls];
-            const float ex = fx - l.x, ey = fy - l.y, ez = fz - l.z;
-            const float d2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
-            const bool in = d2 <= cut2;  // inactive lanes sit at 1e18
-            nevals += active;
-            const unsigned bm = __ballot_sync(0xffffffffu, in);
-            if (in) {
-              const int pos = (head + __popc(bm & lt_mask)) & (kRing - 1);
-              rd2[pos] = d2;
-              rbase[pos] = row + __float_as_int(l.w);
-              rpid[pos] = (slot << 13) | ls;
-            }
-            head += __popc(bm);
-            __syncwarp();
-            if (head - tail >= 64) drain(64);
-          }
+          const bool cand = ax * ax + ay * ay + az * az <= reach2;
+          const unsigned am = __ballot_sync(0xffffffffu, cand);
+          if (cand) W.cand_slot[ncand + __popc(am & lt_mask)] = sb + lane;
+          ncand += __popc(am);
+          if (ncand >= 32) batch(32);
         }
       }
+      if (ncand > 0) batch(ncand);
+      while (head - tail > 0) drain(min(64, head - tail));
+      __syncwarp();
     }
-    while (head - tail > 0) drain(min(64, head - tail));
     // FP64 block reduction of the compensated per-thread sums
     double v = (double)ks - (double)kc;
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -313,6 +371,7 @@ __global__ void __launch_bounds__(kWarps * 32, 5) dfire_score_mixed_kernel(Score
   if (ncut) atomicAdd(&sh_cut, ncut);
   if (npairs) atomicAdd(&sh_pairs, npairs);
   if (nevals) atomicAdd(&sh_evals, nevals);
+  if (nguard) atomicAdd(&ctl->stats[ST_GUARD], nguard);
   __syncthreads();
   if (tid == 0) {
     if (n_done) atomicAdd(&ctl->stats[ST_SCORED], n_done);

@@ -41,6 +41,7 @@ def test_scores_all_precisions(c0, tables):
         sc, en = dk.score_poses(0, poses, sd.SD_PREC_MIXED)
         assert rel_err(en, ref_en).max() <= MIXED_TOL
         assert rel_err(sc, ref_sc).max() <= MIXED_TOL
+        assert dk.stats()["guard_errors"] == 0
 
 
 def test_bins_bit_exact(c0, tables):
@@ -72,6 +73,7 @@ def test_gso_trajectory_fp64_bit_exact(c0, tables):
         stats = dk.stats()
     assert stats["steps"] == steps
     assert stats["edge_u_zero"] == 0 and stats["edge_shortfall"] == 0
+    assert stats["guard_errors"] == 0
 
 
 def test_gso_step_locked_mixed(c0, tables):
@@ -99,6 +101,7 @@ def test_gso_step_locked_mixed(c0, tables):
             oracle_step(osys, st, U[:, t, :], score_override=g.scoring)
             for f, o in STATE_FIELDS:
                 assert np.array_equal(getattr(g, f), getattr(st, o)), f"step {t}: {f} differs"
+        assert dk.stats()["guard_errors"] == 0
 
 
 def test_multi_complex_batch_fp64(tables):
@@ -135,3 +138,20 @@ def test_errors_are_status_codes(c0, tables):
         with pytest.raises(sd.SparkleError) as e:
             dk.score_poses(0, bad.reshape(-1, c0.pose_len)[:2])
         assert e.value.code == 5
+
+
+def test_multi_complex_batch_mixed_scores(tables):
+    """Batched complexes of uneven sizes in one persistent launch (mixed): every rescored pose
+    of one GSO step within 1e-5 of the FP64 oracle."""
+    cxs = [sd.SyntheticComplex(757, 481, 2, 40, seed=51), sd.SyntheticComplex(2039, 1440, 1, 40, seed=52),
+           sd.SyntheticComplex(6143, 633, 1, 40, seed=53)]
+    with sd.Docking(cxs, tables, precision=sd.SD_PREC_MIXED) as dk:
+        for i, c in enumerate(cxs):
+            dk.init_state(i, c.poses)
+            dk.set_draws(i, sd.gso_draws(9 + i, c.n_swarms, 1, c.n_glowworms))
+        dk.step(1)
+        for i, c in enumerate(cxs):
+            g = dk.get_state(i)
+            ref_sc, _ = oracle_scores(OracleSystem(c, tables), c.poses)
+            assert rel_err(g.scoring.ravel(), ref_sc).max() <= MIXED_TOL, f"complex {i}"
+        assert dk.stats()["guard_errors"] == 0
