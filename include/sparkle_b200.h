@@ -171,6 +171,21 @@ int sd_set_precision(sd_ctx* ctx, int precision);
 int sd_score_poses(sd_ctx* ctx, int complex_idx, const double* poses, int n, int precision,
                    double* score_out, double* energy_out);
 
+/* sd_score_poses without any allocation during the call, for callers that must not allocate
+ * device memory while they score (work recorded into a CUDA graph by stream capture, or a
+ * host framework whose memory manager owns all device memory in its steady state).  No
+ * counterpart in the reference.  Inputs and outputs are the caller's DEVICE buffers on the
+ * context's device: d_poses [n][pose_len], d_score [n], d_energy [n] (may be NULL), d_ref [n][3]
+ * (ligand reference points).  n <= 65536 per call, else SD_ERR_ARG.  The scoring kernel's
+ * bookkeeping (work list, counters, descriptor copy) lives in a 288 KiB file-scope device
+ * array that every GPU loading this library holds until exit; all calls on a device share it
+ * and each call rewrites it first, so calls whose GPU work overlaps (other streams or contexts
+ * on the same device) race and must be ordered by the caller.  Runs on the context stream,
+ * asynchronously unless sync != 0.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream capture. */
+int sd_score_poses_noalloc(sd_ctx* ctx, int complex_idx, const double* d_poses, int n, int precision,
+                           double* d_score, double* d_energy, double* d_ref, int sync);
+
 /* Per-pair DFIRE bins of one pose (debug / parity): bins_out[i*n_lig + j] = table bin 0..19,
  * -1 when d^2 > 225.  Receptor order i and ligand order j are the caller's. */
 int sd_dfire_bins(sd_ctx* ctx, int complex_idx, const double* pose, int precision, int* bins_out);

@@ -91,6 +91,8 @@ SIGNATURES = {
     "sd_get_stats": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     "sd_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
     "sd_score_poses": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_int, C.c_int, _dp, _dp]),
+    "sd_score_poses_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                         C.c_void_p, C.c_void_p, C.c_int]),
     "sd_dfire_bins": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_int, _ip]),
     "sd_pydock_grad": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_int, C.c_int, _dp, _dp]),
     "sd_write_gso_output": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp, _ip, _dp,

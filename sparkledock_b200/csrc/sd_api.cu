@@ -465,6 +465,31 @@ int enqueue_step(sd_ctx* c, int precision, int grid, size_t sm) {
 
 }  // namespace
 
+namespace sd {
+// Read-only view of a context for sd_score_poses_noalloc (sd_noalloc.cu): the device
+// descriptor of one complex, table pointers and the launch shape of the scoring kernel.
+// Makes the context's device current; allocates nothing.
+int ctx_noalloc_view(sd_ctx* c, int ci, int precision, DevComplex* desc, ScoreLaunch* L, int* grid, size_t* smem,
+                     int* device, cudaStream_t* stream, int* scoring) {
+  if (!c || ci < 0 || ci >= c->ncplx) return fail(SD_ERR_ARG, "sd_score_poses_noalloc: bad context or complex");
+  if (precision < SD_PREC_FP64_REF || precision > SD_PREC_MIXED)
+    return fail(SD_ERR_ARG, "sd_score_poses_noalloc: unknown precision");
+  SD_CUDA(cudaSetDevice(c->device));
+  int rc = configure_score(c, precision, grid, smem);
+  if (rc) return rc;
+  *desc = c->cx[ci].d;
+  memset(L, 0, sizeof *L);
+  L->table64 = c->d_table64;
+  L->table32 = c->d_table32;
+  L->lj_eps = c->d_lj_eps;
+  L->lj_sigma = c->d_lj_sigma;
+  *device = c->device;
+  *stream = c->stream;
+  *scoring = c->scoring;
+  return SD_OK;
+}
+}  // namespace sd
+
 extern "C" {
 
 const char* sd_last_error(void) { return g_err.c_str(); }
