@@ -125,7 +125,8 @@ def run_gpu(cfg, prec_name, steps, warmup, device, flush, seed=0):
     torch.cuda.synchronize(device)
     ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
     s1 = dk.stats()
-    out = {"ms": ms, "scored": s1["scored_poses"] - s0["scored_poses"], "stats": s1, "ctx": dk, "cxs": cxs}
+    out = {"ms": ms, "scored": s1["scored_poses"] - s0["scored_poses"], "stats": s1, "ctx": dk, "cxs": cxs,
+           "tuning": dk.tuning()}
     return out
 
 
@@ -296,6 +297,7 @@ def main():
     t_ms, scored = reduce_max_sum(dist, sum(run["ms"]), run["scored"], device)
     value = scored / (t_ms / 1e3)
     stats = run["stats"]
+    tuning = run["tuning"]
     run["ctx"].close()
 
     extra = {}
@@ -332,6 +334,7 @@ def main():
                 "d2h_bytes_per_step": e2e["d2h"], "wall_s": e2e["wall_s"]},
         "clocks": clocks,
         "mixed_vs_fp64": {k: {**v, "speedup_mixed": value / v["value"]} for k, v in extra.items()},
+        "autotuner": tuning,
         "edge_counts": {k: stats[k] for k in ("pairs_fallback", "edge_d2_zero", "edge_d2_cutoff", "edge_u_zero",
                                               "edge_shortfall")},
         "per_scored_pose": {"pairs_in_cutoff": stats["pairs_in_cutoff"] / max(1, stats["scored_poses"]),

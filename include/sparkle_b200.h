@@ -162,6 +162,12 @@ int sd_set_draws(sd_ctx* ctx, int complex_idx, const double* u, int n_steps);
 int sd_step(sd_ctx* ctx, int n_steps, int sync);
 
 int sd_get_stats(sd_ctx* ctx, sd_stats* out);
+/* Autotuner result for the mixed-precision DFIRE kernel: the chosen compiled variant, its warps
+ * per CTA and minimum resident CTAs per SM, and (if ms != NULL) the measured time of each
+ * variant on the context's poses (0 before the first mixed sd_step).  The tuner runs once per
+ * context before its first mixed step; SPARKLE_TUNE=0 disables it, SPARKLE_MIXED_VARIANT=k
+ * forces a variant. */
+int sd_get_tuning(sd_ctx* ctx, int* variant, int* warps, int* min_blocks, double* ms, int n_ms);
 int sd_set_precision(sd_ctx* ctx, int precision);
 
 /* Score n arbitrary poses of one complex ([n][pose_len], host): score (reference sign

@@ -179,6 +179,12 @@ class Docking:
     def step(self, n: int = 1, sync: bool = True):
         check(_abi.lib().sd_step(self._ctx, n, 1 if sync else 0), "sd_step")
 
+    def tuning(self) -> dict:
+        v, w, mb = C.c_int(), C.c_int(), C.c_int()
+        ms = np.zeros(8)
+        check(_abi.lib().sd_get_tuning(self._ctx, C.byref(v), C.byref(w), C.byref(mb), dptr(ms), 8), "sd_get_tuning")
+        return {"variant": v.value, "warps": w.value, "min_blocks": mb.value, "ms": [float(x) for x in ms if x]}
+
     def set_precision(self, precision: int):
         check(_abi.lib().sd_set_precision(self._ctx, precision), "sd_set_precision")
 

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -136,6 +137,10 @@ struct sd_ctx {
   int score_threads = 256;
   int score_grid = 0;
   size_t score_smem = 0;
+  // autotuner state (mixed-precision DFIRE kernel variants)
+  int mixed_variant = 0;
+  bool tuned = false;
+  double tune_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 };
 
 namespace {
@@ -413,10 +418,10 @@ int rebuild_worklist(sd_ctx* c) {
   return SD_OK;
 }
 
-int configure_score(sd_ctx* c, int precision, int* grid, size_t* smem) {
+int configure_score_v(sd_ctx* c, int precision, int variant, int* grid, size_t* smem) {
   const size_t sm = score_smem_bytes(precision, c->scoring, c->max_nr, c->max_nl);
-  const void* k = score_kernel_ptr(precision, c->scoring);
-  const int threads = score_threads_of(precision, c->scoring);
+  const void* k = score_kernel_ptr(precision, c->scoring, variant);
+  const int threads = score_threads_of(precision, c->scoring, variant);
   SD_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(sm, 1)));
   int per_sm = 0;
   SD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, sm));
@@ -424,6 +429,118 @@ int configure_score(sd_ctx* c, int precision, int* grid, size_t* smem) {
   *grid = per_sm * c->nsm;
   *smem = sm;
   c->score_threads = threads;
+  return SD_OK;
+}
+
+int configure_score(sd_ctx* c, int precision, int* grid, size_t* smem) {
+  return configure_score_v(c, precision, c->mixed_variant, grid, smem);
+}
+
+// Autotuner: times every compiled variant of the mixed DFIRE kernel (warps per CTA x resident
+// CTAs per SM) on up to 16384 of the context's current poses, twice each, and keeps the fastest
+// for this context.  Results are cached per (device, largest receptor, largest ligand).
+// SPARKLE_TUNE=0 keeps the default variant; SPARKLE_MIXED_VARIANT=k forces variant k.
+int autotune_mixed(sd_ctx* c) {
+  c->tuned = true;
+  const int nv = mixed_variant_count();
+  if (const char* f = getenv("SPARKLE_MIXED_VARIANT")) {
+    const int v = atoi(f);
+    if (v >= 0 && v < nv) c->mixed_variant = v;
+    return SD_OK;
+  }
+  if (const char* t = getenv("SPARKLE_TUNE"))
+    if (atoi(t) == 0) return SD_OK;
+  struct Key {
+    int dev, nr, nl;
+  };
+  static std::vector<std::pair<Key, int>> cache;
+  for (auto& e : cache)
+    if (e.first.dev == c->device && e.first.nr == c->max_nr && e.first.nl == c->max_nl) {
+      c->mixed_variant = e.second;
+      return SD_OK;
+    }
+  // sample poses of every complex into the stateless scratch
+  const int per = std::max(1, 16384 / c->ncplx);
+  std::vector<int> counts(c->ncplx), offs(c->ncplx);
+  int total = 0;
+  size_t pos_bytes = 0;
+  for (int ci = 0; ci < c->ncplx; ++ci) {
+    const DevComplex& D = c->cx[ci].d;
+    counts[ci] = std::min(per, D.S * D.G);
+    offs[ci] = total;
+    total += counts[ci];
+    pos_bytes = std::max(pos_bytes, (size_t)D.pl * 8);
+  }
+  int rc;
+  if ((rc = ensure(c, c->s_pose, (size_t)total * pos_bytes))) return rc;
+  if ((rc = ensure(c, c->s_score, (size_t)total * 8))) return rc;
+  if ((rc = ensure(c, c->s_energy, (size_t)total * 8))) return rc;
+  if ((rc = ensure(c, c->s_ref, (size_t)total * 24))) return rc;
+  if ((rc = ensure(c, c->s_work, (size_t)total * 4))) return rc;
+  std::vector<int> work(total);
+  std::vector<DevComplex> scratch(c->ncplx);
+  for (int ci = 0; ci < c->ncplx; ++ci) {
+    const DevComplex& D = c->cx[ci].d;
+    DevComplex S = D;
+    S.pos = (double*)((char*)c->s_pose.p + (size_t)offs[ci] * pos_bytes);
+    S.scoring = (double*)c->s_score.p + offs[ci];
+    S.ref = (double*)c->s_ref.p + 3 * (size_t)offs[ci];
+    scratch[ci] = S;
+    SD_CUDA(cudaMemcpyAsync(S.pos, D.pos, (size_t)counts[ci] * D.pl * 8, cudaMemcpyDeviceToDevice, c->stream));
+    for (int i = 0; i < counts[ci]; ++i) work[offs[ci] + i] = wi_pack(ci, i);
+  }
+  SD_CUDA(cudaMemcpyAsync(c->d_cplx_scratch, scratch.data(), sizeof(DevComplex) * c->ncplx, cudaMemcpyHostToDevice,
+                          c->stream));
+  SD_CUDA(cudaMemcpyAsync(c->s_work.p, work.data(), (size_t)total * 4, cudaMemcpyHostToDevice, c->stream));
+  StepCtl ctl;
+  SD_CUDA(cudaStreamSynchronize(c->stream));
+  SD_CUDA(cudaMemcpy(&ctl, c->d_ctl_scratch, sizeof ctl, cudaMemcpyDeviceToHost));
+  ctl.count[0] = total;
+  ctl.count[1] = 0;
+  ctl.parity = 0;
+  ScoreLaunch L{};
+  L.cplx = c->d_cplx_scratch;
+  L.ctl = c->d_ctl_scratch;
+  L.work[0] = L.work[1] = (const int*)c->s_work.p;
+  L.table64 = c->d_table64;
+  L.table32 = c->d_table32;
+  L.lj_eps = c->d_lj_eps;
+  L.lj_sigma = c->d_lj_sigma;
+  cudaEvent_t e0, e1;
+  SD_CUDA(cudaEventCreate(&e0));
+  SD_CUDA(cudaEventCreate(&e1));
+  int best = 0;
+  double best_ms = 1e300;
+  for (int v = 0; v < nv && v < 8; ++v) {
+    int grid;
+    size_t sm;
+    if (configure_score_v(c, SD_PREC_MIXED, v, &grid, &sm) != SD_OK) {
+      c->tune_ms[v] = -1;
+      continue;
+    }
+    double vbest = 1e300;
+    for (int rep = 0; rep < 3; ++rep) {
+      ctl.grab[0] = ctl.grab[1] = 0;
+      SD_CUDA(cudaMemcpyAsync(c->d_ctl_scratch, &ctl, sizeof ctl, cudaMemcpyHostToDevice, c->stream));
+      SD_CUDA(cudaEventRecord(e0, c->stream));
+      if ((rc = score_launch(L, SD_PREC_MIXED, c->scoring, grid, c->score_threads, sm, c->stream, v)))
+        return fail(rc, std::string("autotune launch: ") + cudaGetErrorString(cudaGetLastError()));
+      SD_CUDA(cudaEventRecord(e1, c->stream));
+      SD_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      SD_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      vbest = std::min(vbest, (double)ms);
+    }
+    c->tune_ms[v] = vbest;
+    if (vbest < best_ms) {
+      best_ms = vbest;
+      best = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->mixed_variant = best;
+  cache.push_back({Key{c->device, c->max_nr, c->max_nl}, best});
   return SD_OK;
 }
 
@@ -439,7 +556,7 @@ int enqueue_step(sd_ctx* c, int precision, int grid, size_t sm) {
   L.lj_eps = c->d_lj_eps;
   L.lj_sigma = c->d_lj_sigma;
   L.energy_out = nullptr;
-  if ((rc = score_launch(L, precision, c->scoring, grid, c->score_threads, sm, c->stream)))
+  if ((rc = score_launch(L, precision, c->scoring, grid, c->score_threads, sm, c->stream, c->mixed_variant)))
     return fail(rc, std::string("score kernel launch: ") + cudaGetErrorString(cudaGetLastError()));
   GsoLaunch G{};
   G.cplx = c->d_cplx;
@@ -470,7 +587,7 @@ namespace sd {
 // descriptor of one complex, table pointers and the launch shape of the scoring kernel.
 // Makes the context's device current; allocates nothing.
 int ctx_noalloc_view(sd_ctx* c, int ci, int precision, DevComplex* desc, ScoreLaunch* L, int* grid, size_t* smem,
-                     int* device, cudaStream_t* stream, int* scoring) {
+                     int* device, cudaStream_t* stream, int* scoring, int* variant) {
   if (!c || ci < 0 || ci >= c->ncplx) return fail(SD_ERR_ARG, "sd_score_poses_noalloc: bad context or complex");
   if (precision < SD_PREC_FP64_REF || precision > SD_PREC_MIXED)
     return fail(SD_ERR_ARG, "sd_score_poses_noalloc: unknown precision");
@@ -486,6 +603,7 @@ int ctx_noalloc_view(sd_ctx* c, int ci, int precision, DevComplex* desc, ScoreLa
   *device = c->device;
   *stream = c->stream;
   *scoring = c->scoring;
+  *variant = c->mixed_variant;
   return SD_OK;
 }
 }  // namespace sd
@@ -750,6 +868,10 @@ int sd_step(sd_ctx* c, int n_steps, int sync) {
     if (h.draws_used + n_steps > h.d.draw_steps)
       return fail(SD_ERR_STATE, "sd_step: not enough random draws set (sd_set_draws)");
   }
+  if (!c->tuned && c->precision == SD_PREC_MIXED && c->scoring == SD_SCORING_DFIRE) {
+    int rc = autotune_mixed(c);
+    if (rc) return rc;
+  }
   if (!c->graph || c->graph_precision != c->precision) {
     if (c->graph) {
       cudaGraphExecDestroy(c->graph);
@@ -797,6 +919,16 @@ int sd_get_stats(sd_ctx* c, sd_stats* out) {
   out->pairs_in_cutoff = (long long)a.stats[ST_PAIRS];
   out->pairs_evaluated = (long long)a.stats[ST_EVALS];
   out->guard_errors = (long long)(a.stats[ST_GUARD] + b.stats[ST_GUARD]);
+  return SD_OK;
+}
+
+int sd_get_tuning(sd_ctx* c, int* variant, int* warps, int* min_blocks, double* ms, int n_ms) {
+  if (!c) return fail(SD_ERR_ARG, "sd_get_tuning: NULL context");
+  if (variant) *variant = c->mixed_variant;
+  if (warps) *warps = mixed_variant_warps(c->mixed_variant);
+  if (min_blocks) *min_blocks = mixed_variant_min_blocks(c->mixed_variant);
+  if (ms)
+    for (int v = 0; v < n_ms; ++v) ms[v] = v < mixed_variant_count() && c->tuned ? c->tune_ms[v] : 0.0;
   return SD_OK;
 }
 
@@ -854,7 +986,7 @@ int sd_score_poses(sd_ctx* c, int ci, const double* poses, int n, int precision,
   L.lj_eps = c->d_lj_eps;
   L.lj_sigma = c->d_lj_sigma;
   L.energy_out = (double*)c->s_energy.p;
-  if ((rc = score_launch(L, precision, c->scoring, grid, c->score_threads, sm, c->stream)))
+  if ((rc = score_launch(L, precision, c->scoring, grid, c->score_threads, sm, c->stream, c->mixed_variant)))
     return fail(rc, std::string("score kernel: ") + cudaGetErrorString(cudaGetLastError()));
   SD_CUDA(cudaMemcpyAsync(score_out, c->s_score.p, (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));
   if (energy_out)

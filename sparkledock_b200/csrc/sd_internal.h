@@ -122,10 +122,13 @@ struct GsoLaunch {
 
 // kernel launchers (sd_score.cu, sd_gso.cu)
 int score_launch(const ScoreLaunch& L, int precision, int scoring, int grid, int threads, size_t smem,
-                 cudaStream_t st);
+                 cudaStream_t st, int variant);
 size_t score_smem_bytes(int precision, int scoring, int max_nr, int max_nl);
-int score_threads_of(int precision, int scoring);
-const void* score_kernel_ptr(int precision, int scoring);
+int score_threads_of(int precision, int scoring, int variant);
+const void* score_kernel_ptr(int precision, int scoring, int variant);
+int mixed_variant_count();
+int mixed_variant_warps(int v);
+int mixed_variant_min_blocks(int v);
 int gso_launch(const GsoLaunch& L, int threads, cudaStream_t st);
 int bins_launch(const DevComplex* cplx, int c, const double* d_pose, int precision, int* d_bins, int nr, int nl,
                 int* d_fallback, cudaStream_t st);

@@ -26,7 +26,7 @@
 namespace sd {
 // defined in sd_api.cu: the parts of a context this call reads (no allocation)
 int ctx_noalloc_view(sd_ctx* c, int ci, int precision, DevComplex* desc, ScoreLaunch* L, int* grid, size_t* smem,
-                     int* device, cudaStream_t* stream, int* scoring);
+                     int* device, cudaStream_t* stream, int* scoring, int* variant);
 }  // namespace sd
 
 using namespace sd;
@@ -74,10 +74,10 @@ extern "C" int sd_score_poses_noalloc(sd_ctx* ctx, int complex_idx, const double
                                 std::to_string(kMaxPoses) + " per call");
   DevComplex desc;
   ScoreLaunch L{};
-  int grid = 0, device = 0, scoring = SD_SCORING_DFIRE;
+  int grid = 0, device = 0, scoring = SD_SCORING_DFIRE, variant = 0;
   size_t smem = 0;
   cudaStream_t stream = nullptr;
-  int rc = ctx_noalloc_view(ctx, complex_idx, precision, &desc, &L, &grid, &smem, &device, &stream, &scoring);
+  int rc = ctx_noalloc_view(ctx, complex_idx, precision, &desc, &L, &grid, &smem, &device, &stream, &scoring, &variant);
   if (rc) return rc;
   if (n == 0) return SD_OK;
   if (device < 0 || device >= 64) return fail(SD_ERR_ARG, "sd_score_poses_noalloc: device index above 63");
@@ -106,7 +106,8 @@ extern "C" int sd_score_poses_noalloc(sd_ctx* ctx, int complex_idx, const double
   L.work[0] = reinterpret_cast<const int*>(scratch + kCtlBytes + kDescBytes);
   L.work[1] = L.work[0];
   L.energy_out = d_energy;
-  if ((rc = score_launch(L, precision, scoring, grid, score_threads_of(precision, scoring), smem, stream)))
+  if ((rc = score_launch(L, precision, scoring, grid, score_threads_of(precision, scoring, variant), smem, stream,
+                         variant)))
     return fail(rc, std::string("sd_score_poses_noalloc: scoring kernel: ") + cudaGetErrorString(cudaGetLastError()));
   if (sync) {
     e = cudaStreamSynchronize(stream);

@@ -347,27 +347,31 @@ size_t score_smem_bytes(int precision, int scoring, int max_nr, int max_nl) {
          (size_t)4 * ((max_nr + SD_TILE - 1) / SD_TILE);
 }
 
-int score_threads_of(int precision, int scoring) {
+int mixed_variant_count() { return kNumMixedVariants; }
+int mixed_variant_warps(int v) { return kMixedVariants[v < 0 || v >= kNumMixedVariants ? 0 : v].warps; }
+int mixed_variant_min_blocks(int v) { return kMixedVariants[v < 0 || v >= kNumMixedVariants ? 0 : v].min_blocks; }
+
+int score_threads_of(int precision, int scoring, int variant) {
   if (scoring == SD_SCORING_PYDOCK) return pydock_threads();
-  return precision == SD_PREC_MIXED ? kWarps * 32 : 256;
+  return precision == SD_PREC_MIXED ? mixed_variant_warps(variant) * 32 : 256;
 }
 
-const void* score_kernel_ptr(int precision, int scoring) {
+const void* score_kernel_ptr(int precision, int scoring, int variant) {
   if (scoring == SD_SCORING_PYDOCK) return pydock_kernel_ptr(precision, false);
   switch (precision) {
     case SD_PREC_FP64_REF: return (const void*)dfire_score_kernel<SD_PREC_FP64_REF>;
     case SD_PREC_FP64: return (const void*)dfire_score_kernel<SD_PREC_FP64>;
-    default: return (const void*)dfire_score_mixed_kernel;
+    default: return kMixedVariants[variant < 0 || variant >= kNumMixedVariants ? 0 : variant].fn;
   }
 }
 
 int score_launch(const ScoreLaunch& L, int precision, int scoring, int grid, int threads, size_t smem,
-                 cudaStream_t st) {
+                 cudaStream_t st, int variant) {
   if (scoring == SD_SCORING_PYDOCK) return pydock_launch(L, precision, false, nullptr, grid, smem, st);
   switch (precision) {
     case SD_PREC_FP64_REF: dfire_score_kernel<SD_PREC_FP64_REF><<<grid, threads, smem, st>>>(L); break;
     case SD_PREC_FP64: dfire_score_kernel<SD_PREC_FP64><<<grid, threads, smem, st>>>(L); break;
-    default: dfire_score_mixed_kernel<<<grid, threads, smem, st>>>(L); break;
+    default: launch_mixed_variant(variant, L, grid, smem, st); break;
   }
   return cudaGetLastError() == cudaSuccess ? SD_OK : SD_ERR_CUDA;
 }

@@ -22,13 +22,13 @@
 namespace sd {
 namespace {
 
-constexpr int kWarps = 4;
 constexpr int kRing = 1024;  // per-warp ring of in-cutoff pairs (a batch adds at most 32*32)
 
 struct __align__(16) WarpBufs {
   float4 cand_xyz[32];   // staged candidate ligand atoms (centred FP32, col bits)
   int cand_slot[64];     // pending candidate ligand slots
-  float4 rec[32];        // this tile's receptor atoms (centred FP32, row bits)
+  float rx[32], ry[32], rz[32];  // this tile's receptor atoms (centred FP32); SoA: one bank per lane
+  int rrow[32];
   int ring[kRing];       // packed (ligand slot << 5 | lane)
 };
 
@@ -88,7 +88,8 @@ __device__ __forceinline__ bool pair_value(const PoseCtx& P, float d2, int base,
 
 }  // namespace
 
-__global__ void __launch_bounds__(kWarps * 32, 4) dfire_score_mixed_kernel(ScoreLaunch L) {
+template <int kWarps, int kMinBlocks>
+__global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_kernel(ScoreLaunch L) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ WarpBufs wb[kWarps];
   __shared__ double sh_pose[7 + 2 * SD_MAX_MODES];
@@ -227,7 +228,10 @@ __global__ void __launch_bounds__(kWarps * 32, 4) dfire_score_mixed_kernel(Score
         fz = (float)(rz - tz);
         row = C.r_row[slot];
       }
-      W.rec[lane] = make_float4(fx, fy, fz, __int_as_float(row));
+      W.rx[lane] = fx;
+      W.ry[lane] = fy;
+      W.rz[lane] = fz;
+      W.rrow[lane] = row;
       const int nact = __popc(__ballot_sync(0xffffffffu, active));
       int ncand = 0, head = 0, tail = 0;  // warp-uniform
 
@@ -243,10 +247,10 @@ __global__ void __launch_bounds__(kWarps * 32, 4) dfire_score_mixed_kernel(Score
           if ((unsigned)ls >= (unsigned)nls) {  // guard: never taken unless the ring is corrupt
             ++nguard;
           } else {
-          const float4 R = W.rec[rl], Lg = ligS[ls];
-          const float ex = R.x - Lg.x, ey = R.y - Lg.y, ez = R.z - Lg.z;
+          const float4 Lg = ligS[ls];
+          const float ex = W.rx[rl] - Lg.x, ey = W.ry[rl] - Lg.y, ez = W.rz[rl] - Lg.z;
           const float d2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
-          k0 = pair_value(P, d2, __float_as_int(R.w) + __float_as_int(Lg.w), k * SD_TILE + rl, ls, a0, nfb, nz, ncut);
+          k0 = pair_value(P, d2, W.rrow[rl] + __float_as_int(Lg.w), k * SD_TILE + rl, ls, a0, nfb, nz, ncut);
           }
         }
         if (v1) {
@@ -255,10 +259,10 @@ __global__ void __launch_bounds__(kWarps * 32, 4) dfire_score_mixed_kernel(Score
           if ((unsigned)ls >= (unsigned)nls) {  // guard: never taken unless the ring is corrupt
             ++nguard;
           } else {
-          const float4 R = W.rec[rl], Lg = ligS[ls];
-          const float ex = R.x - Lg.x, ey = R.y - Lg.y, ez = R.z - Lg.z;
+          const float4 Lg = ligS[ls];
+          const float ex = W.rx[rl] - Lg.x, ey = W.ry[rl] - Lg.y, ez = W.rz[rl] - Lg.z;
           const float d2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
-          k1 = pair_value(P, d2, __float_as_int(R.w) + __float_as_int(Lg.w), k * SD_TILE + rl, ls, a1, nfb, nz, ncut);
+          k1 = pair_value(P, d2, W.rrow[rl] + __float_as_int(Lg.w), k * SD_TILE + rl, ls, a1, nfb, nz, ncut);
           }
         }
         if (k0) {
@@ -380,6 +384,30 @@ __global__ void __launch_bounds__(kWarps * 32, 4) dfire_score_mixed_kernel(Score
     if (sh_cut) atomicAdd(&ctl->stats[ST_D2CUT], sh_cut);
     if (sh_pairs) atomicAdd(&ctl->stats[ST_PAIRS], sh_pairs);
     if (sh_evals) atomicAdd(&ctl->stats[ST_EVALS], sh_evals);
+  }
+}
+
+// compiled variants of the mixed kernel (warps per CTA, minimum resident CTAs per SM);
+// the host autotuner times them on the context's own poses and keeps the fastest
+struct MixedVariant {
+  const void* fn;
+  int warps;
+  int min_blocks;
+};
+static const MixedVariant kMixedVariants[] = {
+    {(const void*)dfire_score_mixed_kernel<4, 4>, 4, 4},
+    {(const void*)dfire_score_mixed_kernel<4, 5>, 4, 5},
+    {(const void*)dfire_score_mixed_kernel<8, 2>, 8, 2},
+    {(const void*)dfire_score_mixed_kernel<8, 3>, 8, 3},
+};
+constexpr int kNumMixedVariants = sizeof(kMixedVariants) / sizeof(kMixedVariants[0]);
+
+inline void launch_mixed_variant(int v, const ScoreLaunch& L, int grid, size_t smem, cudaStream_t st) {
+  switch (v) {
+    case 1: dfire_score_mixed_kernel<4, 5><<<grid, 128, smem, st>>>(L); break;
+    case 2: dfire_score_mixed_kernel<8, 2><<<grid, 256, smem, st>>>(L); break;
+    case 3: dfire_score_mixed_kernel<8, 3><<<grid, 256, smem, st>>>(L); break;
+    default: dfire_score_mixed_kernel<4, 4><<<grid, 128, smem, st>>>(L); break;
   }
 }
 
