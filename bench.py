@@ -97,7 +97,7 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
 
 
-def run_gpu(cfg, prec_name, steps, warmup, device, flush, seed=0):
+def run_gpu(cfg, prec_name, steps, warmup, device, flush, seed=0, per_step=False):
     """Device-timed run: draws resident in HBM, per-step CUDA events on the context stream,
     L2 flushed (256 MB write) between timed steps outside the events."""
     import torch
@@ -115,6 +115,7 @@ def run_gpu(cfg, prec_name, steps, warmup, device, flush, seed=0):
     s0 = dk.stats()
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    scored_steps = []
     with torch.cuda.stream(stream):
         for k in range(steps):
             if flush is not None:
@@ -122,11 +123,14 @@ def run_gpu(cfg, prec_name, steps, warmup, device, flush, seed=0):
             starts[k].record(stream)
             dk.step(1, sync=False)
             ends[k].record(stream)
+            if per_step:  # synchronises between steps (outside the timed events)
+                scored_steps.append(dk.stats()["scored_poses"])
     torch.cuda.synchronize(device)
     ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
     s1 = dk.stats()
     out = {"ms": ms, "scored": s1["scored_poses"] - s0["scored_poses"], "stats": s1, "ctx": dk, "cxs": cxs,
-           "tuning": dk.tuning()}
+           "tuning": dk.tuning(),
+           "per_step": [b - a for a, b in zip([s0["scored_poses"]] + scored_steps, scored_steps)] if per_step else None}
     return out
 
 
@@ -250,6 +254,7 @@ def main():
     ap.add_argument("--precision", default="", choices=["", "mixed", "fp64", "fp64_ref"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--per-step", action="store_true", help="record scored poses and time of every timed step")
     args = ap.parse_args()
     cfg = dict(CONFIGS[args.config])
     if args.swarms:
@@ -292,7 +297,7 @@ def main():
 
     barrier()
     with Clocks(device) as clk:
-        run = run_gpu(cfg, cfg["precision"], args.steps, args.warmup, device, flush)
+        run = run_gpu(cfg, cfg["precision"], args.steps, args.warmup, device, flush, per_step=args.per_step)
     barrier()
     t_ms, scored = reduce_max_sum(dist, sum(run["ms"]), run["scored"], device)
     value = scored / (t_ms / 1e3)
@@ -335,6 +340,7 @@ def main():
         "clocks": clocks,
         "mixed_vs_fp64": {k: {**v, "speedup_mixed": value / v["value"]} for k, v in extra.items()},
         "autotuner": tuning,
+        **({"per_step": {"scored_poses": run["per_step"], "ms": run["ms"]}} if args.per_step else {}),
         "edge_counts": {k: stats[k] for k in ("pairs_fallback", "edge_d2_zero", "edge_d2_cutoff", "edge_u_zero",
                                               "edge_shortfall")},
         "per_scored_pose": {"pairs_in_cutoff": stats["pairs_in_cutoff"] / max(1, stats["scored_poses"]),

@@ -437,7 +437,7 @@ int configure_score(sd_ctx* c, int precision, int* grid, size_t* smem) {
 }
 
 // Autotuner: times every compiled variant of the mixed DFIRE kernel (warps per CTA x resident
-// CTAs per SM) on up to 16384 of the context's current poses, twice each, and keeps the fastest
+// CTAs per SM) on up to 16384 of the context's current poses, three times each, keeps the fastest
 // for this context.  Results are cached per (device, largest receptor, largest ligand).
 // SPARKLE_TUNE=0 keeps the default variant; SPARKLE_MIXED_VARIANT=k forces variant k.
 int autotune_mixed(sd_ctx* c) {

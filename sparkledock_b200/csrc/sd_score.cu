@@ -20,6 +20,7 @@
 //    per-pair bin unless d2 lies within a proven error bound B of a bin or cutoff edge, in
 //    which case the pair is recomputed in FP64 exactly (counted); compensated (Kahan) FP32
 //    partial sums; FP64 block reduction.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "sd_internal.h"

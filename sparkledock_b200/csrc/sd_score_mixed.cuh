@@ -26,6 +26,7 @@ constexpr int kRing = 1024;  // per-warp ring of in-cutoff pairs (a batch adds a
 
 struct __align__(16) WarpBufs {
   float4 cand_xyz[32];   // staged candidate ligand atoms (centred FP32, col bits)
+  __half cand_h[16][8];  // FP16 pre-filter: per candidate pair {x0,x1,y0,y1,z0,z1,-,-}, tile-centred
   int cand_slot[64];     // pending candidate ligand slots
   float rx[32], ry[32], rz[32];  // this tile's receptor atoms (centred FP32); SoA: one bank per lane
   int rrow[32];
@@ -88,7 +89,12 @@ __device__ __forceinline__ bool pair_value(const PoseCtx& P, float d2, int base,
 
 }  // namespace
 
-template <int kWarps, int kMinBlocks>
+// kH16: stage 1 tests candidate pairs two at a time in packed FP16 on tile-centred coordinates
+// against 229 A^2, a superset of the FP32 test (FP16 error on d^2 <= 1.75 A^2 for pairs within
+// the cutoff: |coordinates| <= 22.5 A after centring, 2^-11 rounding per conversion and
+// subtraction, half an ulp of 256 per multiply-add); stage 2 recomputes d^2 in FP32 and keeps
+// only d^2 <= 225 + B, so the result is identical to the FP32 pre-filter.
+template <int kWarps, int kMinBlocks, bool kH16>
 __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_kernel(ScoreLaunch L) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ WarpBufs wb[kWarps];
@@ -250,7 +256,8 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
           const float4 Lg = ligS[ls];
           const float ex = W.rx[rl] - Lg.x, ey = W.ry[rl] - Lg.y, ez = W.rz[rl] - Lg.z;
           const float d2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
-          k0 = pair_value(P, d2, W.rrow[rl] + __float_as_int(Lg.w), k * SD_TILE + rl, ls, a0, nfb, nz, ncut);
+          if (d2 <= cut2)
+            k0 = pair_value(P, d2, W.rrow[rl] + __float_as_int(Lg.w), k * SD_TILE + rl, ls, a0, nfb, nz, ncut);
           }
         }
         if (v1) {
@@ -262,7 +269,8 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
           const float4 Lg = ligS[ls];
           const float ex = W.rx[rl] - Lg.x, ey = W.ry[rl] - Lg.y, ez = W.rz[rl] - Lg.z;
           const float d2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
-          k1 = pair_value(P, d2, W.rrow[rl] + __float_as_int(Lg.w), k * SD_TILE + rl, ls, a1, nfb, nz, ncut);
+          if (d2 <= cut2)
+            k1 = pair_value(P, d2, W.rrow[rl] + __float_as_int(Lg.w), k * SD_TILE + rl, ls, a1, nfb, nz, ncut);
           }
         }
         if (k0) {
@@ -284,20 +292,63 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
       // stage 1: test the first 32 pending candidates against every lane's receptor atom
       auto batch = [&](int nb) {
         __syncwarp();
-        // unused candidate places sit at -1e18, inactive receptor lanes at +1e18: never in range
-        if (lane < nb) W.cand_xyz[lane] = ligS[W.cand_slot[lane]];
-        else W.cand_xyz[lane] = make_float4(-1e18f, -1e18f, -1e18f, 0.f);
-        __syncwarp();
         unsigned m = 0;
+        if (!kH16) {
+          // unused candidate places sit at -1e18, inactive receptor lanes at +1e18: never in range
+          if (lane < nb) W.cand_xyz[lane] = ligS[W.cand_slot[lane]];
+          else W.cand_xyz[lane] = make_float4(-1e18f, -1e18f, -1e18f, 0.f);
+          __syncwarp();
 #pragma unroll
-        for (int b = 0; b < 32; ++b) {
-          const float4 l = W.cand_xyz[b];
-          const float ex = fx - l.x, ey = fy - l.y, ez = fz - l.z;
-          const float d2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
-          m |= (d2 <= cut2 ? 1u : 0u) << b;
+          for (int b = 0; b < 32; ++b) {
+            const float4 l = W.cand_xyz[b];
+            const float ex = fx - l.x, ey = fy - l.y, ez = fz - l.z;
+            const float d2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
+            m |= (d2 <= cut2 ? 1u : 0u) << b;
+          }
+          // only real candidates and real receptor atoms may produce pairs
+          m &= active ? (nb >= 32 ? 0xffffffffu : ((1u << nb) - 1u)) : 0u;
+        } else {
+          // candidate 2i in the low half, 2i+1 in the high half of pair slot i; unused places
+          // at -1000 and inactive receptor lanes at +inf (1e18 overflows): never in range
+          __half hx = __float2half_rn(-1000.f), hy = hx, hz = hx;
+          if (lane < nb) {
+            const float4 l = ligS[W.cand_slot[lane]];
+            hx = __float2half_rn(l.x - cx);
+            hy = __float2half_rn(l.y - cy);
+            hz = __float2half_rn(l.z - cz);
+          }
+          __half* q = W.cand_h[lane >> 1];
+          q[0 + (lane & 1)] = hx;
+          q[2 + (lane & 1)] = hy;
+          q[4 + (lane & 1)] = hz;
+          __syncwarp();
+          const __half2 rx2 = __half2half2(__float2half_rn(fx - cx));
+          const __half2 ry2 = __half2half2(__float2half_rn(fy - cy));
+          const __half2 rz2 = __half2half2(__float2half_rn(fz - cz));
+          const __half2 th2 = __float2half2_rn(229.0f);
+          unsigned M = 0;
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const uint4 qq = *reinterpret_cast<const uint4*>(W.cand_h[i]);
+            const __half2 dx = __hsub2(rx2, *reinterpret_cast<const __half2*>(&qq.x));
+            const __half2 dy = __hsub2(ry2, *reinterpret_cast<const __half2*>(&qq.y));
+            const __half2 dz = __hsub2(rz2, *reinterpret_cast<const __half2*>(&qq.z));
+            const __half2 d2 = __hfma2(dz, dz, __hfma2(dy, dy, __hmul2(dx, dx)));
+            M |= __hle2_mask(d2, th2) & (0x00010001u << i);
+          }
+          // back to candidate order: bit i -> 2i, bit 16+i -> 2i+1
+          unsigned lo = M & 0xffffu, hi = M >> 16;
+          lo = (lo | (lo << 8)) & 0x00ff00ffu;
+          lo = (lo | (lo << 4)) & 0x0f0f0f0fu;
+          lo = (lo | (lo << 2)) & 0x33333333u;
+          lo = (lo | (lo << 1)) & 0x55555555u;
+          hi = (hi | (hi << 8)) & 0x00ff00ffu;
+          hi = (hi | (hi << 4)) & 0x0f0f0f0fu;
+          hi = (hi | (hi << 2)) & 0x33333333u;
+          hi = (hi | (hi << 1)) & 0x55555555u;
+          m = lo | (hi << 1);
+          m &= active ? (nb >= 32 ? 0xffffffffu : ((1u << nb) - 1u)) : 0u;
         }
-        // only real candidates and real receptor atoms may produce pairs
-        m &= active ? (nb >= 32 ? 0xffffffffu : ((1u << nb) - 1u)) : 0u;
         nevals += (unsigned long long)(lane == 0 ? nb * nact : 0);
         // exclusive scan of the per-lane pair counts
         const int cnt = __popc(m);
@@ -395,19 +446,25 @@ struct MixedVariant {
   int min_blocks;
 };
 static const MixedVariant kMixedVariants[] = {
-    {(const void*)dfire_score_mixed_kernel<4, 4>, 4, 4},
-    {(const void*)dfire_score_mixed_kernel<4, 5>, 4, 5},
-    {(const void*)dfire_score_mixed_kernel<8, 2>, 8, 2},
-    {(const void*)dfire_score_mixed_kernel<8, 3>, 8, 3},
+    {(const void*)dfire_score_mixed_kernel<4, 4, false>, 4, 4},
+    {(const void*)dfire_score_mixed_kernel<4, 5, false>, 4, 5},
+    {(const void*)dfire_score_mixed_kernel<8, 2, false>, 8, 2},
+    {(const void*)dfire_score_mixed_kernel<4, 4, true>, 4, 4},
+    {(const void*)dfire_score_mixed_kernel<4, 5, true>, 4, 5},
+    {(const void*)dfire_score_mixed_kernel<8, 2, true>, 8, 2},
 };
 constexpr int kNumMixedVariants = sizeof(kMixedVariants) / sizeof(kMixedVariants[0]);
+// variants 3..5 use the packed-FP16 pre-filter in stage 1
+inline bool mixed_variant_h16(int v) { return v >= 3; }
 
 inline void launch_mixed_variant(int v, const ScoreLaunch& L, int grid, size_t smem, cudaStream_t st) {
   switch (v) {
-    case 1: dfire_score_mixed_kernel<4, 5><<<grid, 128, smem, st>>>(L); break;
-    case 2: dfire_score_mixed_kernel<8, 2><<<grid, 256, smem, st>>>(L); break;
-    case 3: dfire_score_mixed_kernel<8, 3><<<grid, 256, smem, st>>>(L); break;
-    default: dfire_score_mixed_kernel<4, 4><<<grid, 128, smem, st>>>(L); break;
+    case 1: dfire_score_mixed_kernel<4, 5, false><<<grid, 128, smem, st>>>(L); break;
+    case 2: dfire_score_mixed_kernel<8, 2, false><<<grid, 256, smem, st>>>(L); break;
+    case 3: dfire_score_mixed_kernel<4, 4, true><<<grid, 128, smem, st>>>(L); break;
+    case 4: dfire_score_mixed_kernel<4, 5, true><<<grid, 128, smem, st>>>(L); break;
+    case 5: dfire_score_mixed_kernel<8, 2, true><<<grid, 256, smem, st>>>(L); break;
+    default: dfire_score_mixed_kernel<4, 4, false><<<grid, 128, smem, st>>>(L); break;
   }
 }
 

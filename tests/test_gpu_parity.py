@@ -155,3 +155,22 @@ def test_multi_complex_batch_mixed_scores(tables):
             ref_sc, _ = oracle_scores(OracleSystem(c, tables), c.poses)
             assert rel_err(g.scoring.ravel(), ref_sc).max() <= MIXED_TOL, f"complex {i}"
         assert dk.stats()["guard_errors"] == 0
+
+
+@pytest.mark.parametrize("variant", range(6))
+def test_every_mixed_kernel_variant(variant, c0, tables, monkeypatch):
+    """Each compiled variant of the mixed kernel (the autotuner may pick any) scores the first
+    step's poses within 1e-5 of the FP64 oracle, with no index guard firing."""
+    monkeypatch.setenv("SPARKLE_MIXED_VARIANT", str(variant))
+    osys = OracleSystem(c0, tables)
+    ref_sc, _ = oracle_scores(osys, c0.poses)
+    with sd.Docking([c0], tables, precision=sd.SD_PREC_MIXED) as dk:
+        dk.init_state(0, c0.poses)
+        dk.set_draws(0, sd.gso_draws(0, c0.n_swarms, 1, c0.n_glowworms))
+        dk.step(1)
+        assert dk.tuning()["variant"] == variant
+        g = dk.get_state(0)
+        assert rel_err(g.scoring.ravel(), ref_sc).max() <= MIXED_TOL
+        st = dk.stats()
+        assert st["guard_errors"] == 0
+        assert st["pairs_in_cutoff"] > 0
