@@ -1,0 +1,291 @@
+// lightdock_b200: the reference's command line (source/simulation/run_simulation.cc:21-129,
+// `lightdock -f setup.json -s STEPS -l N`) over the C ABI.
+//
+// setup.json keys read as in get_setup (source/prep/src/read_input_structure.cc:6-59):
+//   swarms, glowworms, anm_rec, anm_lig, use_anm, starting_points_seed, and the GSO keys
+//   rho, gamma, beta, initialLuciferin, initialVisionRange, maximumVisionRange,
+//   maximumNeighbors (read but unused by the reference; honoured here, reference defaults when
+//   absent).  Keys added by this build:
+//   "scoring": "dfire" | "pydock"                (absent: dfire)
+//   "precision": "mixed" | "fp64" | "fp64_ref"  (absent: mixed)
+//   "translation_step", "rotation_step", "nmodes_step"   (absent: the reference's 0.5)
+//   "synthetic": {"receptor_atoms": N, "ligand_atoms": M, "seed": s}
+//        seeded synthetic receptor/ligand in place of receptor_pdb / ligand_pdb (PDB parsing,
+//        ANM and swarm placement are setup stages outside this path)
+//   "dfire_table": path of a DCparams-format file (168*168*20 values, one per line);
+//        absent: seeded synthetic table ("table_seed", default 3)
+// -s STEPS is honoured (the reference parses it but runs its compiled STEPS macro).
+// Output: <dir>/swarm_<i>/gso_<STEPS>.out as the reference GPU path writes them.
+#include <unistd.h>
+
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/sparkle_b200.h"
+
+namespace {
+
+// ---- minimal JSON reader (objects, arrays, strings, numbers, true/false/null) ----
+struct JVal {
+  enum Kind { Null, Bool, Num, Str, Arr, Obj } kind = Null;
+  bool b = false;
+  double num = 0;
+  std::string str;
+  std::vector<JVal> arr;
+  std::map<std::string, JVal> obj;
+  const JVal* get(const std::string& k) const {
+    auto it = obj.find(k);
+    return it == obj.end() ? nullptr : &it->second;
+  }
+};
+
+struct JParser {
+  const std::string& s;
+  size_t i = 0;
+  std::string err;
+  explicit JParser(const std::string& t) : s(t) {}
+  void ws() {
+    while (i < s.size() && (s[i] == ' ' || s[i] == '\n' || s[i] == '\t' || s[i] == '\r')) ++i;
+  }
+  bool fail(const std::string& m) {
+    if (err.empty()) err = m + " at offset " + std::to_string(i);
+    return false;
+  }
+  bool value(JVal& v) {
+    ws();
+    if (i >= s.size()) return fail("unexpected end of input");
+    const char c = s[i];
+    if (c == '{') return object(v);
+    if (c == '[') return array(v);
+    if (c == '"') {
+      v.kind = JVal::Str;
+      return string(v.str);
+    }
+    if (!s.compare(i, 4, "true")) {
+      v.kind = JVal::Bool;
+      v.b = true;
+      i += 4;
+      return true;
+    }
+    if (!s.compare(i, 5, "false")) {
+      v.kind = JVal::Bool;
+      i += 5;
+      return true;
+    }
+    if (!s.compare(i, 4, "null")) {
+      v.kind = JVal::Null;
+      i += 4;
+      return true;
+    }
+    char* end = nullptr;
+    v.num = strtod(s.c_str() + i, &end);
+    if (end == s.c_str() + i) return fail("unexpected character");
+    v.kind = JVal::Num;
+    i = end - s.c_str();
+    return true;
+  }
+  bool string(std::string& out) {
+    ++i;
+    while (i < s.size() && s[i] != '"') {
+      if (s[i] == '\\' && i + 1 < s.size()) {
+        const char e = s[i + 1];
+        out += e == 'n' ? '\n' : e == 't' ? '\t' : e;
+        i += 2;
+      } else {
+        out += s[i++];
+      }
+    }
+    if (i >= s.size()) return fail("unterminated string");
+    ++i;
+    return true;
+  }
+  bool array(JVal& v) {
+    v.kind = JVal::Arr;
+    ++i;
+    ws();
+    if (i < s.size() && s[i] == ']') {
+      ++i;
+      return true;
+    }
+    for (;;) {
+      JVal e;
+      if (!value(e)) return false;
+      v.arr.push_back(std::move(e));
+      ws();
+      if (i < s.size() && s[i] == ',') {
+        ++i;
+        continue;
+      }
+      if (i < s.size() && s[i] == ']') {
+        ++i;
+        return true;
+      }
+      return fail("expected , or ]");
+    }
+  }
+  bool object(JVal& v) {
+    v.kind = JVal::Obj;
+    ++i;
+    ws();
+    if (i < s.size() && s[i] == '}') {
+      ++i;
+      return true;
+    }
+    for (;;) {
+      ws();
+      if (i >= s.size() || s[i] != '"') return fail("expected a key");
+      std::string k;
+      if (!string(k)) return false;
+      ws();
+      if (i >= s.size() || s[i] != ':') return fail("expected :");
+      ++i;
+      JVal e;
+      if (!value(e)) return false;
+      v.obj[k] = std::move(e);
+      ws();
+      if (i < s.size() && s[i] == ',') {
+        ++i;
+        continue;
+      }
+      if (i < s.size() && s[i] == '}') {
+        ++i;
+        return true;
+      }
+      return fail("expected , or }");
+    }
+  }
+};
+
+double num_or(const JVal& root, const char* k, double def) {
+  const JVal* v = root.get(k);
+  return v && v->kind == JVal::Num ? v->num : def;
+}
+std::string str_or(const JVal& root, const char* k, const std::string& def) {
+  const JVal* v = root.get(k);
+  return v && v->kind == JVal::Str ? v->str : def;
+}
+
+int die(const std::string& m) {
+  fprintf(stderr, "lightdock_b200: %s\n", m.c_str());
+  return 1;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  std::string file;
+  int steps = 100;  // the reference's STEPS on its GPU path
+  std::string outdir = ".";
+  int device = 0;
+  int ch;
+  while ((ch = getopt(argc, argv, "f:s:l:o:d:")) != -1) {
+    if (ch == 'f') file = optarg;
+    else if (ch == 's') steps = atoi(optarg);
+    else if (ch == 'l') (void)atoi(optarg);  // parsed and unused, as in the reference
+    else if (ch == 'o') outdir = optarg;
+    else if (ch == 'd') device = atoi(optarg);
+    else return die("usage: lightdock_b200 -f setup.json [-s STEPS] [-o DIR] [-d DEVICE]");
+  }
+  if (file.empty()) return die("usage: lightdock_b200 -f setup.json [-s STEPS] [-o DIR] [-d DEVICE]");
+  if (steps <= 0) return die("-s STEPS must be positive");
+  std::ifstream in(file);
+  if (!in) return die("cannot open " + file);
+  std::stringstream ss;
+  ss << in.rdbuf();
+  const std::string text = ss.str();
+  JVal root;
+  JParser jp(text);
+  if (!jp.value(root) || root.kind != JVal::Obj) return die("setup.json: " + (jp.err.empty() ? "not an object" : jp.err));
+
+  const int swarms = (int)num_or(root, "swarms", 0), G = (int)num_or(root, "glowworms", 200);
+  const JVal* ua = root.get("use_anm");
+  const bool use_anm = !ua || ua->kind != JVal::Bool || ua->b;
+  const int anm_rec = use_anm ? (int)num_or(root, "anm_rec", 10) : 0;
+  const int anm_lig = use_anm ? (int)num_or(root, "anm_lig", 10) : 0;
+  if (swarms <= 0) return die("setup.json: \"swarms\" must be a positive number");
+  const std::string scoring_s = str_or(root, "scoring", "dfire"), prec_s = str_or(root, "precision", "mixed");
+  int scoring = scoring_s == "dfire" ? SD_SCORING_DFIRE : scoring_s == "pydock" ? SD_SCORING_PYDOCK : -1;
+  if (scoring < 0) return die("setup.json: \"scoring\" must be \"dfire\" or \"pydock\"");
+  int precision = prec_s == "mixed" ? SD_PREC_MIXED : prec_s == "fp64" ? SD_PREC_FP64 : prec_s == "fp64_ref" ? SD_PREC_FP64_REF : -1;
+  if (precision < 0) return die("setup.json: \"precision\" must be \"mixed\", \"fp64\" or \"fp64_ref\"");
+  const JVal* syn = root.get("synthetic");
+  if (!syn || syn->kind != JVal::Obj)
+    return die("setup.json: PDB inputs (receptor_pdb / ligand_pdb) need the setup stages (PDB parsing, ANM, "
+               "swarm placement) that this path does not include; give a \"synthetic\" block");
+
+  sd_synth_spec spec;
+  spec.n_rec = (int)num_or(*syn, "receptor_atoms", 0);
+  spec.n_lig = (int)num_or(*syn, "ligand_atoms", 0);
+  spec.n_swarms = swarms;
+  spec.n_glowworms = G;
+  spec.n_modes_rec = anm_rec;
+  spec.n_modes_lig = anm_lig;
+  spec.seed = (unsigned long long)num_or(*syn, "seed", num_or(root, "starting_points_seed", 1));
+  long long bytes = 0;
+  if (sd_synth_buffer_size(&spec, &bytes) != SD_OK) return die(sd_last_error());
+  std::unique_ptr<char[]> buf(new char[(size_t)bytes]);
+  sd_complex_desc desc;
+  double* pos0 = nullptr;
+  if (sd_synth_generate(&spec, buf.get(), &desc, &pos0) != SD_OK) return die(sd_last_error());
+
+  const size_t tsz = (size_t)SD_DFIRE_TYPES * SD_DFIRE_TYPES * SD_DFIRE_BINS;
+  std::vector<double> table(tsz), eps(SD_LJ_TYPES), sig(SD_LJ_TYPES);
+  sd_synth_tables((unsigned long long)num_or(root, "table_seed", 3), table.data(), eps.data(), sig.data());
+  const std::string tpath = str_or(root, "dfire_table", "");
+  if (!tpath.empty()) {  // DCparams format (prepare_gso_tasks.cc:1175-1189): one value per line
+    std::ifstream tf(tpath);
+    if (!tf) return die("cannot open dfire_table " + tpath);
+    std::string line;
+    size_t k = 0;
+    while (std::getline(tf, line) && k < tsz) table[k++] = strtod(line.c_str(), nullptr);
+    if (k != tsz) return die("dfire_table " + tpath + ": expected 564480 values");
+  }
+  sd_tables tables = {table.data(), eps.data(), sig.data()};
+  sd_gso_params p;
+  sd_gso_params_default(&p);
+  p.rho = num_or(root, "rho", p.rho);
+  p.gamma = num_or(root, "gamma", p.gamma);
+  p.beta = num_or(root, "beta", p.beta);
+  p.initial_luciferin = num_or(root, "initialLuciferin", p.initial_luciferin);
+  p.initial_vision_range = num_or(root, "initialVisionRange", p.initial_vision_range);
+  p.max_vision_range = num_or(root, "maximumVisionRange", p.max_vision_range);
+  p.max_neighbors = (int)num_or(root, "maximumNeighbors", p.max_neighbors);
+  p.translation_step = num_or(root, "translation_step", p.translation_step);
+  p.rotation_step = num_or(root, "rotation_step", p.rotation_step);
+  p.nmodes_step = num_or(root, "nmodes_step", p.nmodes_step);
+
+  sd_ctx* ctx = nullptr;
+  if (sd_ctx_create(&desc, 1, &tables, &p, scoring, precision, device, &ctx) != SD_OK) return die(sd_last_error());
+  const auto t0 = std::chrono::steady_clock::now();
+  std::vector<double> u((size_t)swarms * steps * G);
+  sd_gso_draws(0, swarms, steps, G, u.data());  // the reference CPU path's serial mt19937(0)
+  int rc = sd_init_state(ctx, 0, pos0);
+  if (!rc) rc = sd_set_draws(ctx, 0, u.data(), steps);
+  if (!rc) rc = sd_step(ctx, steps, 1);
+  const int pl = SD_POSE_LEN(anm_rec, anm_lig);
+  const size_t n = (size_t)swarms * G;
+  std::vector<double> pos(n * pl), luc(n), vis(n), sc(n);
+  std::vector<int> nnei(n);
+  sd_swarm_state st = {pos.data(), sc.data(), luc.data(), vis.data(), nullptr, nullptr, nnei.data(), nullptr, nullptr};
+  if (!rc) rc = sd_get_state(ctx, 0, &st);
+  const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  if (rc) {
+    const std::string m = sd_last_error();
+    sd_ctx_destroy(ctx);
+    return die(m);
+  }
+  sd_ctx_destroy(ctx);
+  if (sd_write_gso_output(outdir.c_str(), 0, swarms, G, pl, steps, pos.data(), luc.data(), nnei.data(), vis.data(),
+                          sc.data()) != SD_OK)
+    return die(sd_last_error());
+  printf("simulation execution:%f\n", secs);
+  return 0;
+}

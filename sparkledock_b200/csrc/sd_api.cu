@@ -639,6 +639,24 @@ int sd_ctx_create(const sd_complex_desc* complexes, int n_complexes, const sd_ta
     int rc = check_desc(complexes[i], scoring);
     if (rc) return rc;
   }
+  // device memory the context will hold (tables, per-complex data, state, work lists), checked
+  // against SPARKLE_DEVICE_BUDGET_MB when set (a forced budget, e.g. to test the OOM path)
+  {
+    size_t bytes = (size_t)(SD_TABLE_SIZE + 32) * 12 + 4096;
+    for (int i = 0; i < n_complexes; ++i) {
+      const sd_complex_desc& d = complexes[i];
+      const size_t nr = (size_t)((d.n_rec + SD_TILE - 1) / SD_TILE) * SD_TILE, nl = (size_t)d.n_lig;
+      const size_t n = (size_t)d.n_swarms * d.n_glowworms, pl = SD_POSE_LEN(d.n_modes_rec, d.n_modes_lig);
+      bytes += nr * (24 + 24 * d.n_modes_rec + 20) + nl * (24 + 24 * d.n_modes_lig + 20) * 2;
+      bytes += n * (8 * pl + 8 * 3 + 4 * 4 + 24 + 8);
+    }
+    if (const char* b = getenv("SPARKLE_DEVICE_BUDGET_MB")) {
+      const double budget = atof(b) * 1048576.0;
+      if ((double)bytes > budget)
+        return fail(SD_ERR_OOM, "sd_ctx_create: needs about " + std::to_string(bytes >> 20) +
+                                    " MiB of device memory, over SPARKLE_DEVICE_BUDGET_MB=" + b);
+    }
+  }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     cudaGetLastError();

@@ -86,3 +86,38 @@ def test_gso_output_writer_format(tmp_path):
             exp = "(" + ", ".join("%f" % v for v in pos[s, g]) + ")\t0\t0\t" + "%f" % luc[s, g] + "\t" + \
                   str(nn[s, g]) + "\t" + "%f" % vr[s, g] + "\t" + "%f" % sc[s, g] + "\t"
             assert lines[1 + g] == exp
+
+
+def test_forced_device_budget_gives_oom_status(tables, monkeypatch):
+    """Fault injection on the host: a tiny forced device budget turns context creation into an
+    SD_ERR_OOM status (no device is touched, so this runs without a GPU)."""
+    monkeypatch.setenv("SPARKLE_DEVICE_BUDGET_MB", "1")
+    cx = sd.SyntheticComplex(3002, 1274, 40, 200, seed=1)
+    try:
+        sd.Docking([cx], tables)
+    except sd.SparkleError as e:
+        assert e.code == _abi.SD_ERR_OOM
+        assert "SPARKLE_DEVICE_BUDGET_MB" in str(e)
+    else:
+        raise AssertionError("expected SD_ERR_OOM")
+
+
+def test_invalid_descriptors_are_rejected(tables):
+    """Malformed inputs fail with SD_ERR_ARG / SD_ERR_NUMERIC before any device work."""
+    cx = sd.SyntheticComplex(60, 40, 1, 8, seed=2)
+    bad = sd.SyntheticComplex(60, 40, 1, 8, seed=2)
+    bad.rec_type[3] = 168
+    with __import__("pytest").raises(sd.SparkleError) as e:
+        sd.Docking([bad], tables)
+    assert e.value.code == _abi.SD_ERR_ARG
+    nan = sd.SyntheticComplex(60, 40, 1, 8, seed=2)
+    nan.lig_xyz[0, 0] = float("nan")
+    with __import__("pytest").raises(sd.SparkleError) as e:
+        sd.Docking([nan], tables)
+    assert e.value.code == _abi.SD_ERR_NUMERIC
+    t2 = (tables[0].copy(), tables[1], tables[2])
+    t2[0][5] = float("inf")
+    if sd.device_count() > 0:
+        with __import__("pytest").raises(sd.SparkleError) as e:
+            sd.Docking([cx], t2)
+        assert e.value.code == _abi.SD_ERR_NUMERIC
