@@ -40,6 +40,10 @@ CONFIGS = {
 G = 200
 METRIC = "scored poses/s and GSO steps/s on 1 B200, mixed vs FP64 at <=1e-5 rel energy err"
 L2_FLUSH_BYTES = 256 << 20
+# DRAM bytes per rescored pose of the mixed DFIRE scorer on the single-complex workload, from
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of three full-size launches
+# (profiles/dfire_score_mixed_c1_launches.md)
+DRAM_BYTES_PER_SCORED_POSE = 334.0
 
 
 def make_complexes(cfg, seed0=100):
@@ -129,6 +133,7 @@ def run_gpu(cfg, prec_name, steps, warmup, device, flush, seed=0, per_step=False
     ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
     s1 = dk.stats()
     out = {"ms": ms, "scored": s1["scored_poses"] - s0["scored_poses"], "stats": s1, "ctx": dk, "cxs": cxs,
+           "pairs": s1["pairs_in_cutoff"] - s0["pairs_in_cutoff"],
            "tuning": dk.tuning(),
            "per_step": [b - a for a, b in zip([s0["scored_poses"]] + scored_steps, scored_steps)] if per_step else None}
     return out
@@ -300,8 +305,10 @@ def main():
         run = run_gpu(cfg, cfg["precision"], args.steps, args.warmup, device, flush, per_step=args.per_step)
     barrier()
     t_ms, scored = reduce_max_sum(dist, sum(run["ms"]), run["scored"], device)
+    _, pairs_all = reduce_max_sum(dist, 0.0, run["pairs"], device)  # every rank takes part
     value = scored / (t_ms / 1e3)
     stats = run["stats"]
+    pairs_timed_rank = run["pairs"]
     tuning = run["tuning"]
     run["ctx"].close()
 
@@ -348,9 +355,21 @@ def main():
                             "pairs_brute_force": sum(nr * nl for nr, nl, _ in cfg["complexes"]) / len(cfg["complexes"])},
     }
     if pairs:
-        line["roofline"] = {"bound": "fp32", "achieved": 8.0 * pairs / (t_ms / 1e3) / 1e12, "peak": fp32_peak,
-                            "unit": "TFLOP/s", "frac": 8.0 * pairs / (t_ms / 1e3) / 1e12 / fp32_peak, "traffic": None,
-                            "peak_source": "nominal FP32 vector pipe at the measured max SM clock"}
+        # algorithmic work: 8 flops per receptor-ligand pair inside the 15 A cutoff (the
+        # distance: 3 sub + 3 mul + 2 add), pairs counted by the kernel over every timed step;
+        # bound: the FP32 vector pipe (the kernel is neither HBM- nor tensor-shaped)
+        pairs_timed = pairs_all
+        achieved = 8.0 * pairs_timed / (t_ms / 1e3) / 1e12
+        brute = 8.0 * line["per_scored_pose"]["pairs_brute_force"] * scored / (t_ms / 1e3) / 1e12
+        line["roofline"] = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                            "frac": achieved / fp32_peak,
+                            "traffic": DRAM_BYTES_PER_SCORED_POSE * scored / args.steps,
+                            "traffic_unit": "bytes per launch (DRAM, ncu)",
+                            "peak_source": "nominal FP32 vector pipe (148 SMs x 128 lanes x 2) at the measured "
+                                           f"max SM clock {peaks.get('sm_max_mhz', 1965.0):.0f} MHz "
+                                           f"({peak_src} peaks file has no FP32 vector figure)",
+                            "hbm_frac": DRAM_BYTES_PER_SCORED_POSE * value / 1e9 / peaks.get("hbm_gbs", 6650.0),
+                            "brute_force_equivalent_tflops": brute}
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             line["cpu_baseline"] = {k: v for k, v in cpu_reference_rate(cfg, args.cpu_budget).items()

@@ -54,6 +54,27 @@ struct PoseCtx {
   float B;
 };
 
+// exact FP64 key of one pair near a bin edge or the cutoff (rare: kept out of line so that its
+// registers do not weigh on the hot loop); returns -1 when the pair is outside the cutoff and
+// sets *edge to 1 for d^2 == 0, 2 for d^2 == 225
+__device__ __noinline__ int exact_pair_key(const DevComplex* C, int nslots, const double* pose, const double* q,
+                                           const double* qi, const double* T, int slot, int j, int* edge) {
+  double rx, ry, rz, lx, ly, lz;
+  receptor_exact(*C, nslots, slot, pose, rx, ry, rz);
+  ligand_exact(*C, j, pose, q, qi, lx, ly, lz);
+  const double dx = rx - lx, dy = ry - ly, dz = rz - lz;
+  const double e2 = dx * dx + dy * dy + dz * dz;
+  *edge = 0;
+  if (!(e2 <= SD_CUTOFF2)) return -1;
+  if (e2 == 0.0) {
+    *edge = 1;
+    return 0;
+  }
+  const int key = exact_key_m(e2, T);
+  if (key == 29) *edge = 2;
+  return key;
+}
+
 // value of one in-cutoff candidate pair (slot = receptor slot, ls = ligand chunk slot);
 // returns false when the exact FP64 distance shows the pair is outside the cutoff
 __device__ __forceinline__ bool pair_value(const PoseCtx& P, float d2, int base, int slot, int ls, float& val,
@@ -67,20 +88,11 @@ __device__ __forceinline__ bool pair_value(const PoseCtx& P, float d2, int base,
   const bool near = (d2 - kk.x <= P.B) || (kk.y - d2 <= P.B);
   if (near) {
     ++nfb;
-    const int j = P.C->l_perm[ls];
-    double rx, ry, rz, lx, ly, lz;
-    receptor_exact(*P.C, P.nslots, slot, P.pose, rx, ry, rz);
-    ligand_exact(*P.C, j, P.pose, P.q, P.qi, lx, ly, lz);
-    const double dx = rx - lx, dy = ry - ly, dz = rz - lz;
-    const double e2 = dx * dx + dy * dy + dz * dz;
-    if (!(e2 <= SD_CUTOFF2)) return false;
-    if (e2 == 0.0) {
-      key = 0;
-      ++nz;
-    } else {
-      key = exact_key_m(e2, P.T);
-      if (key == 29) ++ncut;
-    }
+    int edge;
+    key = exact_pair_key(P.C, P.nslots, P.pose, P.q, P.qi, P.T, slot, P.C->l_perm[ls], &edge);
+    if (key < 0) return false;
+    nz += edge == 1;
+    ncut += edge == 2;
     bin = __float_as_int(P.key4[key].z);
   }
   val = P.table[base + bin];
