@@ -36,6 +36,8 @@ CONFIGS = {
                precision="mixed", steps=100),
     "c3": dict(workload="large receptor, mixed precision", complexes=[(17307, 1125, 1245)], precision="mixed",
                steps=50),
+    "c4": dict(workload="pyDock-style energy adjoint (4096 poses) + refinement of the top 5 per swarm",
+               complexes=[(3002, 1274, 402)], precision="mixed", steps=100),
 }
 G = 200
 METRIC = "scored poses/s and GSO steps/s on 1 B200, mixed vs FP64 at <=1e-5 rel energy err"
@@ -136,6 +138,62 @@ def run_gpu(cfg, prec_name, steps, warmup, device, flush, seed=0, per_step=False
            "pairs": s1["pairs_in_cutoff"] - s0["pairs_in_cutoff"],
            "tuning": dk.tuning(),
            "per_step": [b - a for a, b in zip([s0["scored_poses"]] + scored_steps, scored_steps)] if per_step else None}
+    return out
+
+
+def fp64_spot_check(dk, cxs, frac=0.01):
+    """Energies of 1 % of the final poses (at least 256 per complex) from the mixed kernel
+    against the plain FP64 kernel: max |E_mixed - E_fp64| / max(|E_fp64|, 1) on the raw DFIRE
+    sum, and the same on the score (the reference's `energy`, -(0.0157 E - 4.7))."""
+    import sparkledock_b200 as sd
+    worst, worst_sc, n = 0.0, 0.0, 0
+    for i, c in enumerate(cxs):
+        pos = dk.get_state(i).pos.reshape(-1, c.pose_len)
+        k = max(256, int(frac * len(pos)))
+        sel = pos[np.linspace(0, len(pos) - 1, min(k, len(pos))).astype(int)]
+        s32, e32 = dk.score_poses(i, sel, sd.SD_PREC_MIXED)
+        s64, e64 = dk.score_poses(i, sel, sd.SD_PREC_FP64)
+        worst = max(worst, float((np.abs(e32 - e64) / np.maximum(np.abs(e64), 1.0)).max()))
+        worst_sc = max(worst_sc, float((np.abs(s32 - s64) / np.maximum(np.abs(s64), 1.0)).max()))
+        n += len(sel)
+    return {"poses": n, "max_rel_energy_err": worst, "max_rel_score_err": worst_sc, "tolerance": 1e-5}
+
+
+def run_c4(cfg, device, gso_steps, refine_iters=50):
+    """Adjoint throughput and accuracy on 4096 poses, then refinement of the top 5 glowworms per
+    swarm after a DFIRE GSO run, judged by the FP64 pyDock-style energy."""
+    import torch
+    import sparkledock_b200 as sd
+    nr, nl, S = cfg["complexes"][0]
+    cx = sd.SyntheticComplex(nr, nl, S, G, 10, 10, seed=100)
+    tables = sd.synthetic_tables(3)
+    poses = cx.poses.reshape(-1, cx.pose_len)[:4096]
+    out = {}
+    with sd.Docking([cx], tables, scoring=sd.SD_SCORING_PYDOCK, device=device) as dk:
+        for name, prec in (("fp32", sd.SD_PREC_MIXED), ("fp64", sd.SD_PREC_FP64)):
+            dk.pydock_grad(0, poses[:256], prec)
+            torch.cuda.synchronize(device)
+            t0 = time.perf_counter()
+            e, g = dk.pydock_grad(0, poses, prec)
+            dt = time.perf_counter() - t0
+            out[name] = {"poses_per_s": len(poses) / dt, "ms": dt * 1e3, "grad": g}
+        g32, g64 = out["fp32"].pop("grad"), out["fp64"].pop("grad")
+        scale = np.maximum(np.abs(g64).max(axis=1, keepdims=True), 1.0)
+        out["max_rel_grad_err_fp32_vs_fp64"] = float((np.abs(g32 - g64) / scale).max())
+    with sd.Docking([cx], tables, precision=sd.SD_PREC_MIXED, device=device) as dk:
+        dk.init_state(0, cx.poses)
+        dk.set_draws(0, sd.gso_draws(0, S, gso_steps, G))
+        dk.step(gso_steps)
+        st = dk.get_state(0)
+    top = np.argsort(-st.scoring, axis=1)[:, :5]
+    sel = np.stack([st.pos[s, top[s]] for s in range(S)]).reshape(-1, cx.pose_len)
+    with sd.Docking([cx], tables, scoring=sd.SD_SCORING_PYDOCK, device=device) as dk:
+        t0 = time.perf_counter()
+        _, e0, e1 = dk.refine(0, sel, iters=refine_iters, step=0.5)
+        dt = time.perf_counter() - t0
+    out["refinement"] = {"poses": int(len(sel)), "iterations": refine_iters, "seconds": dt,
+                         "mean_fp64_energy_before": float(e0.mean()), "mean_fp64_energy_after": float(e1.mean()),
+                         "fraction_improved": float((e1 < e0).mean()), "max_increase": float((e1 - e0).max())}
     return out
 
 
@@ -272,6 +330,16 @@ def main():
               "anm_modes": [10, 10], "gso_steps": args.warmup + args.steps, "scoring": "dfire",
               "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{args.gpus}"}
 
+    if args.config == "c4":
+        if rank == 0:
+            import torch
+            torch.cuda.set_device(0)
+            res = run_c4(cfg, 0, args.warmup + args.steps)
+            print(json.dumps({"metric": "pyDock-style adjoint poses/s (energy + 26-dim gradient, host buffers)",
+                              "value": res["fp32"]["poses_per_s"], "unit": "poses/s", "n_gpus": 1,
+                              "higher_is_better": True, "data": "synthetic", "config": config, **res}))
+        return
+
     if args.impl == "reference":
         if rank != 0:
             return
@@ -310,6 +378,7 @@ def main():
     stats = run["stats"]
     pairs_timed_rank = run["pairs"]
     tuning = run["tuning"]
+    spot = fp64_spot_check(run["ctx"], run["cxs"]) if cfg["precision"] == "mixed" else None
     run["ctx"].close()
 
     extra = {}
@@ -347,6 +416,7 @@ def main():
         "clocks": clocks,
         "mixed_vs_fp64": {k: {**v, "speedup_mixed": value / v["value"]} for k, v in extra.items()},
         "autotuner": tuning,
+        "fp64_spot_check": spot,
         **({"per_step": {"scored_poses": run["per_step"], "ms": run["ms"]}} if args.per_step else {}),
         "edge_counts": {k: stats[k] for k in ("pairs_fallback", "edge_d2_zero", "edge_d2_cutoff", "edge_u_zero",
                                               "edge_shortfall")},

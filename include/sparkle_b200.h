@@ -211,6 +211,16 @@ int sd_write_gso_output(const char* dir, int swarm_offset, int n_swarms, int n_g
                         int steps, const double* pos, const double* luciferin, const int* nnei_len,
                         const double* vision_range, const double* scoring);
 
+/* Optional post-GSO local refinement (pyDock-scoring contexts; project-defined, no reference
+ * counterpart): `iters` steepest-descent steps on the smooth elec + LJ energy using the GPU
+ * adjoint at `precision`, along the normalised gradient in (t, R_L*w, e_rec, e_lig) coordinates
+ * (R_L the ligand radius, so every component moves in Angstrom-like units), starting at `step`
+ * A.  A step is kept only when the plain FP64 energy of the moved pose is lower (then the
+ * pose's step grows by 1.5x, else it halves), so the FP64 energy never increases.
+ * poses [n][pose_len] in/out (host); energy_before / energy_after [n] FP64 energies (nullable). */
+int sd_refine_poses(sd_ctx* ctx, int complex_idx, double* poses, int n, int iters, double step, int precision,
+                    double* energy_before, double* energy_after);
+
 /* ---- synthetic complexes (seeded), for tests and benchmarks ---- */
 typedef struct {
   int n_rec, n_lig, n_swarms, n_glowworms, n_modes_rec, n_modes_lig;

@@ -209,6 +209,19 @@ class Docking:
         check(_abi.lib().sd_dfire_bins(self._ctx, ci, dptr(pose), precision, iptr(out)), "sd_dfire_bins")
         return out
 
+    def refine(self, ci: int, poses: np.ndarray, iters: int = 50, step: float = 0.5,
+               precision: int = SD_PREC_MIXED):
+        """Post-GSO refinement on the pyDock-style energy; returns (poses, E_before, E_after),
+        FP64 energies, never increasing."""
+        c = self._complexes[ci]
+        p = np.array(poses, np.float64).reshape(-1, c.pose_len).copy()
+        n = p.shape[0]
+        e0 = np.empty(n)
+        e1 = np.empty(n)
+        check(_abi.lib().sd_refine_poses(self._ctx, ci, dptr(p), n, iters, step, precision, dptr(e0), dptr(e1)),
+              "sd_refine_poses")
+        return p, e0, e1
+
     def pydock_grad(self, ci: int, poses: np.ndarray, precision: int = SD_PREC_MIXED):
         c = self._complexes[ci]
         poses = np.ascontiguousarray(poses, np.float64).reshape(-1, c.pose_len)

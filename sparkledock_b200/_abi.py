@@ -98,6 +98,7 @@ SIGNATURES = {
     "sd_pydock_grad": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_int, C.c_int, _dp, _dp]),
     "sd_write_gso_output": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp, _ip, _dp,
                                       _dp]),
+    "sd_refine_poses": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_int, C.c_int, C.c_double, C.c_int, _dp, _dp]),
     "sd_synth_buffer_size": (C.c_int, [C.POINTER(SynthSpec), C.POINTER(C.c_longlong)]),
     "sd_synth_generate": (C.c_int, [C.POINTER(SynthSpec), C.c_void_p, C.POINTER(ComplexDesc),
                                     C.POINTER(_dp)]),

@@ -119,7 +119,6 @@ struct sd_ctx {
   DevComplex* d_cplx = nullptr;
   DevComplex* d_cplx_scratch = nullptr;
   double* d_table64 = nullptr;
-  float* d_table32 = nullptr;
   double* d_lj_eps = nullptr;
   double* d_lj_sigma = nullptr;
   StepCtl* d_ctl = nullptr;
@@ -503,7 +502,6 @@ int autotune_mixed(sd_ctx* c) {
   L.ctl = c->d_ctl_scratch;
   L.work[0] = L.work[1] = (const int*)c->s_work.p;
   L.table64 = c->d_table64;
-  L.table32 = c->d_table32;
   L.lj_eps = c->d_lj_eps;
   L.lj_sigma = c->d_lj_sigma;
   cudaEvent_t e0, e1;
@@ -552,7 +550,6 @@ int enqueue_step(sd_ctx* c, int precision, int grid, size_t sm) {
   L.work[0] = c->d_work[0];
   L.work[1] = c->d_work[1];
   L.table64 = c->d_table64;
-  L.table32 = c->d_table32;
   L.lj_eps = c->d_lj_eps;
   L.lj_sigma = c->d_lj_sigma;
   L.energy_out = nullptr;
@@ -597,7 +594,6 @@ int ctx_noalloc_view(sd_ctx* c, int ci, int precision, DevComplex* desc, ScoreLa
   *desc = c->cx[ci].d;
   memset(L, 0, sizeof *L);
   L->table64 = c->d_table64;
-  L->table32 = c->d_table32;
   L->lj_eps = c->d_lj_eps;
   L->lj_sigma = c->d_lj_sigma;
   *device = c->device;
@@ -705,7 +701,6 @@ int sd_ctx_create(const sd_complex_desc* complexes, int n_complexes, const sd_ta
   if ((rc = cu(cudaMalloc(&c->d_cplx, sizeof(DevComplex) * n_complexes), "cudaMalloc"))) return bail(rc);
   if ((rc = cu(cudaMalloc(&c->d_cplx_scratch, sizeof(DevComplex) * n_complexes), "cudaMalloc"))) return bail(rc);
   if ((rc = cu(cudaMalloc(&c->d_table64, sizeof(double) * (SD_TABLE_SIZE + 32)), "cudaMalloc"))) return bail(rc);
-  if ((rc = cu(cudaMalloc(&c->d_table32, sizeof(float) * (SD_TABLE_SIZE + 32)), "cudaMalloc"))) return bail(rc);
   if ((rc = cu(cudaMalloc(&c->d_lj_eps, sizeof(double) * SD_LJ_TYPES), "cudaMalloc"))) return bail(rc);
   if ((rc = cu(cudaMalloc(&c->d_lj_sigma, sizeof(double) * SD_LJ_TYPES), "cudaMalloc"))) return bail(rc);
   if ((rc = cu(cudaMalloc(&c->d_ctl, sizeof(StepCtl)), "cudaMalloc"))) return bail(rc);
@@ -715,11 +710,9 @@ int sd_ctx_create(const sd_complex_desc* complexes, int n_complexes, const sd_ta
   if ((rc = cu(cudaMalloc(&c->d_swarm_map, sizeof(int) * c->total_swarms), "cudaMalloc"))) return bail(rc);
   {
     std::vector<double> t64(SD_TABLE_SIZE + 32, 0.0);
-    std::vector<float> t32(SD_TABLE_SIZE + 32, 0.f);
     for (int i = 0; i < SD_TABLE_SIZE; ++i) {
       if (!std::isfinite(tables->dfire_energy[i])) return bail(fail(SD_ERR_NUMERIC, "non-finite DFIRE table entry"));
       t64[i] = tables->dfire_energy[i];
-      t32[i] = (float)tables->dfire_energy[i];
     }
     std::vector<double> eps(SD_LJ_TYPES, 0.0), sig(SD_LJ_TYPES, 0.0);
     if (tables->lj_eps && tables->lj_sigma)
@@ -733,7 +726,6 @@ int sd_ctx_create(const sd_complex_desc* complexes, int n_complexes, const sd_ta
     StepCtl ctl;
     memset(&ctl, 0, sizeof ctl);
     if ((rc = cu(cudaMemcpy(c->d_table64, t64.data(), t64.size() * 8, cudaMemcpyHostToDevice), "upload"))) return bail(rc);
-    if ((rc = cu(cudaMemcpy(c->d_table32, t32.data(), t32.size() * 4, cudaMemcpyHostToDevice), "upload"))) return bail(rc);
     if ((rc = cu(cudaMemcpy(c->d_lj_eps, eps.data(), eps.size() * 8, cudaMemcpyHostToDevice), "upload"))) return bail(rc);
     if ((rc = cu(cudaMemcpy(c->d_lj_sigma, sig.data(), sig.size() * 8, cudaMemcpyHostToDevice), "upload"))) return bail(rc);
     if ((rc = cu(cudaMemcpy(c->d_swarm_map, smap.data(), smap.size() * 4, cudaMemcpyHostToDevice), "upload"))) return bail(rc);
@@ -752,7 +744,7 @@ int sd_ctx_destroy(sd_ctx* c) {
   if (c->graph) cudaGraphExecDestroy(c->graph);
   for (auto& h : c->cx)
     for (void* p : h.owned) cudaFree(p);
-  void* ps[] = {c->d_cplx, c->d_cplx_scratch, c->d_table64, c->d_table32, c->d_lj_eps, c->d_lj_sigma, c->d_ctl,
+  void* ps[] = {c->d_cplx, c->d_cplx_scratch, c->d_table64, c->d_lj_eps, c->d_lj_sigma, c->d_ctl,
                 c->d_ctl_scratch, c->d_work[0], c->d_work[1], c->d_swarm_map, c->s_pose.p, c->s_score.p,
                 c->s_ref.p, c->s_energy.p, c->s_work.p, c->s_grad.p, c->s_bins.p};
   for (void* p : ps)
@@ -1000,7 +992,6 @@ int sd_score_poses(sd_ctx* c, int ci, const double* poses, int n, int precision,
   L.work[0] = (const int*)c->s_work.p;
   L.work[1] = (const int*)c->s_work.p;
   L.table64 = c->d_table64;
-  L.table32 = c->d_table32;
   L.lj_eps = c->d_lj_eps;
   L.lj_sigma = c->d_lj_sigma;
   L.energy_out = (double*)c->s_energy.p;
@@ -1081,7 +1072,6 @@ int sd_pydock_grad(sd_ctx* c, int ci, const double* poses, int n, int precision,
   L.work[0] = (const int*)c->s_work.p;
   L.work[1] = (const int*)c->s_work.p;
   L.table64 = c->d_table64;
-  L.table32 = c->d_table32;
   L.lj_eps = c->d_lj_eps;
   L.lj_sigma = c->d_lj_sigma;
   L.energy_out = (double*)c->s_energy.p;
@@ -1091,6 +1081,64 @@ int sd_pydock_grad(sd_ctx* c, int ci, const double* poses, int n, int precision,
     SD_CUDA(cudaMemcpyAsync(energy_out, c->s_energy.p, (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));
   SD_CUDA(cudaMemcpyAsync(grad_out, c->s_grad.p, (size_t)n * ng * 8, cudaMemcpyDeviceToHost, c->stream));
   SD_CUDA(cudaStreamSynchronize(c->stream));
+  return SD_OK;
+}
+
+int sd_refine_poses(sd_ctx* c, int ci, double* poses, int n, int iters, double step, int precision,
+                    double* energy_before, double* energy_after) {
+  if (!c || !poses || n < 0 || iters < 0 || !(step > 0) || ci < 0 || ci >= c->ncplx)
+    return fail(SD_ERR_ARG, "sd_refine_poses: bad arguments");
+  if (c->scoring != SD_SCORING_PYDOCK) return fail(SD_ERR_ARG, "sd_refine_poses: context scoring is not pyDock");
+  if (n == 0) return SD_OK;
+  const DevComplex& D = c->cx[ci].d;
+  const int pl = D.pl, ng = 6 + D.nmr + D.nml;
+  const double RL = std::max(1.0, (double)D.lig_radius);
+  std::vector<double> sc(n), E(n), Ec(n), g((size_t)n * ng), cand((size_t)n * pl), alpha(n, step);
+  int rc;
+  if ((rc = sd_score_poses(c, ci, poses, n, SD_PREC_FP64, sc.data(), E.data()))) return rc;
+  if (energy_before) std::copy(E.begin(), E.end(), energy_before);
+  for (int it = 0; it < iters; ++it) {
+    if ((rc = sd_pydock_grad(c, ci, poses, n, precision, nullptr, g.data()))) return rc;
+    for (int i = 0; i < n; ++i) {
+      const double* gi = g.data() + (size_t)i * ng;
+      const double* p0 = poses + (size_t)i * pl;
+      double* p1 = cand.data() + (size_t)i * pl;
+      std::copy(p0, p0 + pl, p1);
+      double nrm = 0;
+      for (int k = 0; k < ng; ++k) {
+        const double v = (k >= 3 && k < 6) ? gi[k] / RL : gi[k];
+        nrm += v * v;
+      }
+      nrm = std::sqrt(nrm);
+      if (!(nrm > 0) || !std::isfinite(nrm)) continue;
+      const double a = alpha[i] / nrm;
+      for (int k = 0; k < 3; ++k) p1[k] -= a * gi[k];
+      // rotation by the angle vector -a * g_w / RL^2 (arc length a * |g_w| / RL at radius RL)
+      const double w[3] = {-a * gi[3] / (RL * RL), -a * gi[4] / (RL * RL), -a * gi[5] / (RL * RL)};
+      const double th = std::sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+      if (th > 0) {
+        const double s2 = std::sin(0.5 * th) / th, c2 = std::cos(0.5 * th);
+        const double dq[4] = {c2, s2 * w[0], s2 * w[1], s2 * w[2]};
+        const double q[4] = {p1[3], p1[4], p1[5], p1[6]};
+        p1[3] = dq[0] * q[0] - dq[1] * q[1] - dq[2] * q[2] - dq[3] * q[3];
+        p1[4] = dq[0] * q[1] + dq[1] * q[0] + dq[2] * q[3] - dq[3] * q[2];
+        p1[5] = dq[0] * q[2] - dq[1] * q[3] + dq[2] * q[0] + dq[3] * q[1];
+        p1[6] = dq[0] * q[3] + dq[1] * q[2] - dq[2] * q[1] + dq[3] * q[0];
+      }
+      for (int k = 6; k < ng; ++k) p1[7 + (k - 6)] -= a * gi[k];
+    }
+    if ((rc = sd_score_poses(c, ci, cand.data(), n, SD_PREC_FP64, sc.data(), Ec.data()))) return rc;
+    for (int i = 0; i < n; ++i) {
+      if (Ec[i] < E[i]) {
+        std::copy(cand.data() + (size_t)i * pl, cand.data() + (size_t)(i + 1) * pl, poses + (size_t)i * pl);
+        E[i] = Ec[i];
+        alpha[i] *= 1.5;
+      } else {
+        alpha[i] *= 0.5;
+      }
+    }
+  }
+  if (energy_after) std::copy(E.begin(), E.end(), energy_after);
   return SD_OK;
 }
 

@@ -104,7 +104,6 @@ struct ScoreLaunch {
   StepCtl* ctl;
   const int* work[2];
   const double* table64;   // [SD_TABLE_SIZE + 32] zero padded
-  const float* table32;
   const double* lj_eps;    // [20] pyDock
   const double* lj_sigma;
   double* energy_out;      // nullable [local glowworm] raw energies (stateless scoring)

@@ -16,10 +16,10 @@
 //    reference, and the pose energy adds the v_i in ascending original i (zeros skipped:
 //    adding +0.0 never changes a sum), so energies are bit-identical to the reference
 //    order with or without culling;
-//  * MIXED: distances from FP32 coordinates centred on the pose translation, an exact
-//    per-pair bin unless d2 lies within a proven error bound B of a bin or cutoff edge, in
-//    which case the pair is recomputed in FP64 exactly (counted); compensated (Kahan) FP32
-//    partial sums; FP64 block reduction.
+//  * MIXED (sd_score_mixed.cuh): distances from FP32 coordinates centred on the pose
+//    translation, an exact per-pair bin unless d2 lies within a proven error bound B of a bin
+//    or cutoff edge, in which case the pair is recomputed in FP64 exactly (counted); FP64 sums
+//    of the FP64 table values.
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -54,9 +54,6 @@ struct LigD {
   int pad;
 };
 
-template <int PREC>
-struct ScoreSmem;
-
 __device__ __forceinline__ int exact_key(double d2, const double* T) {
   float f = sqrtf((float)d2) * 2.0f - 1.0f;
   int k = (int)f;
@@ -66,20 +63,8 @@ __device__ __forceinline__ int exact_key(double d2, const double* T) {
   return k;
 }
 
-__device__ __forceinline__ double block_sum_double(double v, double* red) {
-  // deterministic: fixed shuffle tree per warp, then warp 0 adds warp sums in order
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  if (lane == 0) red[warp] = v;
-  __syncthreads();
-  double s = 0.0;
-  if (threadIdx.x == 0)
-    for (int w = 0; w < nw; ++w) s += red[w];
-  __syncthreads();
-  return s;  // valid in thread 0
-}
-
-// PREC: SD_PREC_FP64_REF (no culling), SD_PREC_FP64, SD_PREC_MIXED
+// PREC: SD_PREC_FP64_REF (no culling) or SD_PREC_FP64 (culled); the mixed-precision kernel is
+// in sd_score_mixed.cuh
 template <int PREC>
 __global__ void __launch_bounds__(256) dfire_score_kernel(ScoreLaunch L) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -88,14 +73,12 @@ __global__ void __launch_bounds__(256) dfire_score_kernel(ScoreLaunch L) {
   __shared__ double sh_T[32];
   __shared__ float sh_Tf[32];
   __shared__ int sh_lut[32];
-  __shared__ double sh_red[32];
   __shared__ int sh_item;
   __shared__ int sh_ntile, sh_next;
-  __shared__ float sh_bound[4];  // dR, dL, B (mixed), unused
+  __shared__ float sh_bound[4];  // dR, dL
   __shared__ unsigned long long sh_fallback, sh_z, sh_cut, sh_pairs, sh_evals;
 
   constexpr bool kCull = PREC != SD_PREC_FP64_REF;
-  constexpr bool kMixed = PREC == SD_PREC_MIXED;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid < 32) {
     sh_T[tid] = c_T[tid];
@@ -142,10 +125,6 @@ __global__ void __launch_bounds__(256) dfire_score_kernel(ScoreLaunch L) {
       dL = dL * 1.0001f + 1e-4f;
       sh_bound[0] = dR;
       sh_bound[1] = dL;
-      // error bound of the FP32 d2 against the FP64 d2 for pairs within 15.1 A
-      const float RL = C.lig_radius + dL;
-      const float u32 = 5.9604645e-8f;
-      sh_bound[2] = 2.0f * (2.02f * u32 * (26.2f * (2.0f * RL + 15.1f) + 228.0f) + 3.0f * u32 * 228.0f) + 1e-6f;
     }
     __syncthreads();
     // ---- ligand of this pose into shared memory ----
@@ -163,10 +142,9 @@ __global__ void __launch_bounds__(256) dfire_score_kernel(ScoreLaunch L) {
       ligand_exact(C, j, sh_pose, sh_q, sh_qi, x, y, z);
       const int col = C.l_col[j];
       ligF[j] = make_float4((float)(x - tx), (float)(y - ty), (float)(z - tz), __int_as_float(col));
-      if (!kMixed) ligD[j] = LigD{x, y, z, col, 0};
+      ligD[j] = LigD{x, y, z, col, 0};
     }
-    if (!kMixed)
-      for (int i = tid; i < nr; i += blockDim.x) vacc[i] = 0.0;
+    for (int i = tid; i < nr; i += blockDim.x) vacc[i] = 0.0;
     if (tid == 0) {
       // ligand reference point (prepare_gso_tasks.cc:460, :513, :524-526)
       double x = C.lig_ref[0], y = C.lig_ref[1], z = C.lig_ref[2];
@@ -177,7 +155,7 @@ __global__ void __launch_bounds__(256) dfire_score_kernel(ScoreLaunch L) {
       ref[2] = z + tz;
     }
     __syncthreads();
-    const float dR = sh_bound[0], dL = sh_bound[1], B = sh_bound[2];
+    const float dR = sh_bound[0], dL = sh_bound[1];
     const float tile_reach_base = 15.0f + dR + SD_CULL_MARGIN;
     const float lig_reach = C.lig_radius + dL;
     for (int k = tid; k < C.ntiles; k += blockDim.x) {
@@ -193,8 +171,6 @@ __global__ void __launch_bounds__(256) dfire_score_kernel(ScoreLaunch L) {
     }
     __syncthreads();
     const int ntile = sh_ntile;
-    float ks = 0.f, kc = 0.f;  // MIXED per-thread Kahan state across tiles
-    unsigned long long nfb = 0;
 
     for (;;) {
       int ti = 0;
@@ -216,7 +192,6 @@ __global__ void __launch_bounds__(256) dfire_score_kernel(ScoreLaunch L) {
         receptor_exact(C, nslots, slot, sh_pose, rx, ry, rz);
         row = C.r_row[slot];
       }
-      const float fx = (float)(rx - tx), fy = (float)(ry - ty), fz = (float)(rz - tz);
       double v = 0.0;  // FP64 partial of receptor atom `orig`
       for (int base = 0; base < nl; base += 32) {
         const int j = base + lane;
@@ -232,7 +207,7 @@ __global__ void __launch_bounds__(256) dfire_score_kernel(ScoreLaunch L) {
           mask &= mask - 1;
           const int jj = base + b;
           n_evals += active;
-          if (!kMixed) {
+          {
             const LigD l = ligD[jj];
             const double ddx = rx - l.x, ddy = ry - l.y, ddz = rz - l.z;
             const double d2 = ddx * ddx + ddy * ddy + ddz * ddz;
@@ -248,53 +223,14 @@ __global__ void __launch_bounds__(256) dfire_score_kernel(ScoreLaunch L) {
               v += L.table64[row + l.col + sh_lut[key]];
               ++n_pairs;
             }
-          } else {
-            const float4 l = ligF[jj];
-            const float ex = fx - l.x, ey = fy - l.y, ez = fz - l.z;
-            const float d2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
-            if (active && d2 <= 225.0f + B) {
-              float f = sqrtf(d2) * 2.0f - 1.0f;
-              int key = (int)f;
-              key = key < 0 ? 0 : (key > 29 ? 29 : key);
-              const bool near = (d2 - sh_Tf[key] <= B) || (sh_Tf[key + 1] - d2 <= B);
-              float val = 0.f;
-              bool in = true;
-              if (near) {
-                // exact FP64 recomputation of this pair
-                double lx, ly, lz;
-                ligand_exact(C, jj, sh_pose, sh_q, sh_qi, lx, ly, lz);
-                const double ddx = rx - lx, ddy = ry - ly, ddz = rz - lz;
-                const double e2 = ddx * ddx + ddy * ddy + ddz * ddz;
-                ++nfb;
-                in = e2 <= SD_CUTOFF2;
-                if (in) {
-                  if (e2 == 0.0) {
-                    key = 0;
-                    atomicAdd(&sh_z, 1ull);
-                  } else {
-                    key = exact_key(e2, sh_T);
-                    if (key == 29) atomicAdd(&sh_cut, 1ull);
-                  }
-                }
-              }
-              if (in) {
-                ++n_pairs;
-                val = L.table32[row + __float_as_int(l.w) + sh_lut[key]];
-                const float y = val - kc;
-                const float t = ks + y;
-                kc = (t - ks) - y;
-                ks = t;
-              }
-            }
           }
         }
       }
-      if (!kMixed && active) vacc[orig] = v;
+      if (active) vacc[orig] = v;
     }
-    if (kMixed && nfb) atomicAdd(&sh_fallback, nfb);
     __syncthreads();
     double E;
-    if (!kMixed) {
+    {
       // reference order: E += v_i for i ascending (zero partials skipped)
       E = 0.0;
       if (warp == 0) {
@@ -308,8 +244,6 @@ __global__ void __launch_bounds__(256) dfire_score_kernel(ScoreLaunch L) {
           }
         }
       }
-    } else {
-      E = block_sum_double((double)ks - (double)kc, sh_red);
     }
     if (tid == 0) {
       const double score = ((E)*0.0157 - 4.7) * -1;

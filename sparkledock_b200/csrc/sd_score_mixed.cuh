@@ -1,4 +1,4 @@
-// Mixed-precision DFIRE scoring (FP32 distances, exact bins, compensated FP32 sums).
+// Mixed-precision DFIRE scoring (FP16/FP32 distances, exact bins, FP64 sums of table values).
 // Included by sd_score.cu (shares its constant-memory key thresholds and bin table).
 //
 // Same contract as the FP64 kernels in sd_score.cu (energy of cdfire_calculate_dfire,
@@ -14,7 +14,11 @@
 //    in-cutoff pairs (ligand slot, lane) to a per-warp ring;
 //  * stage 2 drains the ring 64 pairs at a time, two per lane: recompute d^2 (same FP32
 //    expression, so the same value), key from a fast reciprocal square root, the exact-bin
-//    guard against the proven FP32 error bound B, two table gathers in flight, Kahan sums.
+//    guard against the proven FP32 error bound B, two table gathers in flight, and each lane
+//    adds the FP64 table value of its pairs with one FP64 add.  The FP64 pipe is otherwise
+//    idle here; compensated FP32 (Kahan) sums were measured to leave ~2e-5 absolute error at
+//    60k pairs per pose, because every compensation step rounds the incoming value, and they
+//    cost five FP32 adds per pair.
 //    Pairs within B of a bin edge or of the cutoff are recomputed from the exact FP64 pose
 //    transform (counted as fallbacks).
 #pragma once
@@ -50,7 +54,7 @@ struct PoseCtx {
   const double* qi;
   const double* T;
   const float4* key4;  // per key: {lower threshold, upper threshold, bin bits, 0}
-  const float* table;
+  const double* table;  // FP64 DFIRE table: one 8-byte gather per pair
   float B;
 };
 
@@ -77,7 +81,7 @@ __device__ __noinline__ int exact_pair_key(const DevComplex* C, int nslots, cons
 
 // value of one in-cutoff candidate pair (slot = receptor slot, ls = ligand chunk slot);
 // returns false when the exact FP64 distance shows the pair is outside the cutoff
-__device__ __forceinline__ bool pair_value(const PoseCtx& P, float d2, int base, int slot, int ls, float& val,
+__device__ __forceinline__ bool pair_value(const PoseCtx& P, float d2, int base, int slot, int ls, double& val,
                                            unsigned long long& nfb, unsigned long long& nz, unsigned long long& ncut) {
   // key estimate; d2 == 0 gives NaN -> 0 and is caught by the edge guard below
   const float r = d2 * rsqrtf(d2);
@@ -219,9 +223,9 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
     }
     __syncthreads();
     const int ntile = sh_ntile;
-    PoseCtx P{&C, nslots, sh_pose, sh_q, sh_qi, sh_T, sh_key4, L.table32, sh_bound[2]};
+    PoseCtx P{&C, nslots, sh_pose, sh_q, sh_qi, sh_T, sh_key4, L.table64, sh_bound[2]};
     const float cut2 = 225.0f + P.B;
-    float ks = 0.f, kc = 0.f;
+    double acc = 0.0;  // per-thread FP64 sum of the table values of its pairs
 
     for (;;) {
       int ti = 0;
@@ -257,7 +261,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
       auto drain = [&](int n) {
         const int i0 = tail + lane, i1 = tail + 32 + lane;
         const bool v0 = lane < n, v1 = lane + 32 < n;
-        float a0 = 0.f, a1 = 0.f;
+        double a0 = 0.0, a1 = 0.0;
         bool k0 = false, k1 = false;
         if (v0) {
           const int e = W.ring[i0 & (kRing - 1)];
@@ -286,17 +290,11 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
           }
         }
         if (k0) {
-          const float y = a0 - kc;
-          const float t = ks + y;
-          kc = (t - ks) - y;
-          ks = t;
+          acc += a0;
           ++npairs;
         }
         if (k1) {
-          const float y = a1 - kc;
-          const float t = ks + y;
-          kc = (t - ks) - y;
-          ks = t;
+          acc += a1;
           ++npairs;
         }
         tail += n;
@@ -419,8 +417,8 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
       while (head - tail > 0) drain(min(64, head - tail));
       __syncwarp();
     }
-    // FP64 block reduction of the compensated per-thread sums
-    double v = (double)ks - (double)kc;
+    // FP64 block reduction of the per-thread sums
+    double v = acc;
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     if (lane == 0) sh_red[warp] = v;
     __syncthreads();
