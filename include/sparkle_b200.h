@@ -56,7 +56,7 @@ extern "C" {
 /* precision / algorithm of the pair stage */
 #define SD_PREC_FP64_REF 0   /* FP64, all Nr*Nl pairs, reference pair order: bit-exact energies */
 #define SD_PREC_FP64 1       /* FP64 with the cutoff cell culling; same order -> bit-exact */
-#define SD_PREC_MIXED 2      /* FP32 distances + compensated FP32 sums, FP64 near-boundary fallback */
+#define SD_PREC_MIXED 2      /* FP16/FP32 distances, exact bins (FP64 near-edge fallback), FP64 sums */
 
 /* One receptor/ligand complex and its swarms.  Mirrors the fields of the reference's
  * Complex (source/prep/include/complex.h:10-104: atom_coordinates, mask, modes, num_atoms)
@@ -168,6 +168,9 @@ int sd_get_stats(sd_ctx* ctx, sd_stats* out);
  * context before its first mixed step; SPARKLE_TUNE=0 disables it, SPARKLE_MIXED_VARIANT=k
  * forces a variant. */
 int sd_get_tuning(sd_ctx* ctx, int* variant, int* warps, int* min_blocks, double* ms, int n_ms);
+/* Number of compiled variants of the mixed-precision DFIRE kernel (valid SPARKLE_MIXED_VARIANT
+ * values are 0 .. count-1; sd_get_tuning reports one time per variant). */
+int sd_mixed_variant_count(void);
 int sd_set_precision(sd_ctx* ctx, int precision);
 
 /* Score n arbitrary poses of one complex ([n][pose_len], host): score (reference sign

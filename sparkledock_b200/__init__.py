@@ -16,7 +16,7 @@ from . import _abi
 from ._abi import (SD_PREC_FP64, SD_PREC_FP64_REF, SD_PREC_MIXED, SD_SCORING_DFIRE,  # noqa: F401
                    SD_SCORING_PYDOCK, SparkleError, check, dptr, iptr)
 
-__all__ = ["SyntheticComplex", "synthetic_tables", "gso_draws", "GsoParams", "Docking",
+__all__ = ["SyntheticComplex", "synthetic_tables", "gso_draws", "mixed_variant_count", "GsoParams", "Docking",
            "SD_PREC_FP64_REF", "SD_PREC_FP64", "SD_PREC_MIXED", "SD_SCORING_DFIRE",
            "SD_SCORING_PYDOCK", "SparkleError", "device_count"]
 
@@ -25,6 +25,11 @@ def device_count() -> int:
     n = C.c_int(0)
     check(_abi.lib().sd_device_count(C.byref(n)), "sd_device_count")
     return n.value
+
+
+def mixed_variant_count() -> int:
+    """Number of compiled variants of the mixed-precision DFIRE kernel (autotuner candidates)."""
+    return int(_abi.lib().sd_mixed_variant_count())
 
 
 def gso_draws(seed: int, n_swarms: int, n_steps: int, n_glowworms: int) -> np.ndarray:
@@ -181,9 +186,10 @@ class Docking:
 
     def tuning(self) -> dict:
         v, w, mb = C.c_int(), C.c_int(), C.c_int()
-        ms = np.zeros(8)
-        check(_abi.lib().sd_get_tuning(self._ctx, C.byref(v), C.byref(w), C.byref(mb), dptr(ms), 8), "sd_get_tuning")
-        return {"variant": v.value, "warps": w.value, "min_blocks": mb.value, "ms": [float(x) for x in ms if x]}
+        n = mixed_variant_count()
+        ms = np.zeros(n)
+        check(_abi.lib().sd_get_tuning(self._ctx, C.byref(v), C.byref(w), C.byref(mb), dptr(ms), n), "sd_get_tuning")
+        return {"variant": v.value, "warps": w.value, "min_blocks": mb.value, "ms": [float(x) for x in ms]}
 
     def set_precision(self, precision: int):
         check(_abi.lib().sd_set_precision(self._ctx, precision), "sd_set_precision")

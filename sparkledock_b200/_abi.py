@@ -90,6 +90,7 @@ SIGNATURES = {
     "sd_step": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "sd_get_stats": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     "sd_get_tuning": (C.c_int, [C.c_void_p, _ip, _ip, _ip, _dp, C.c_int]),
+    "sd_mixed_variant_count": (C.c_int, []),
     "sd_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
     "sd_score_poses": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_int, C.c_int, _dp, _dp]),
     "sd_score_poses_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p,

@@ -139,7 +139,7 @@ struct sd_ctx {
   // autotuner state (mixed-precision DFIRE kernel variants)
   int mixed_variant = 0;
   bool tuned = false;
-  double tune_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double tune_ms[SD_MAX_VARIANTS] = {};
 };
 
 namespace {
@@ -509,7 +509,7 @@ int autotune_mixed(sd_ctx* c) {
   SD_CUDA(cudaEventCreate(&e1));
   int best = 0;
   double best_ms = 1e300;
-  for (int v = 0; v < nv && v < 8; ++v) {
+  for (int v = 0; v < nv && v < SD_MAX_VARIANTS; ++v) {
     int grid;
     size_t sm;
     if (configure_score_v(c, SD_PREC_MIXED, v, &grid, &sm) != SD_OK) {
@@ -941,6 +941,8 @@ int sd_get_tuning(sd_ctx* c, int* variant, int* warps, int* min_blocks, double* 
     for (int v = 0; v < n_ms; ++v) ms[v] = v < mixed_variant_count() && c->tuned ? c->tune_ms[v] : 0.0;
   return SD_OK;
 }
+
+int sd_mixed_variant_count(void) { return mixed_variant_count(); }
 
 int sd_set_precision(sd_ctx* c, int precision) {
   if (!c || precision < SD_PREC_FP64_REF || precision > SD_PREC_MIXED)

@@ -19,6 +19,7 @@
 #define SD_MAX_REC 24576        /* receptor atoms (FP64 per-atom partials in shared memory) */
 #define SD_MAX_G 1024           /* glowworms per swarm (one thread each) */
 #define SD_CULL_MARGIN 0.05f    /* A, covers FP32 rounding of the conservative culling tests */
+#define SD_MAX_VARIANTS 16      /* compiled variants of the mixed DFIRE kernel (autotuner) */
 #define SD_NOALLOC_MAX_POSES 65536           /* poses per sd_score_poses_noalloc call */
 #define SD_NOALLOC_SCRATCH_BYTES (288 * 1024) /* its file-scope device scratch array */
 

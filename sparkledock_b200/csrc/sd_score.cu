@@ -268,8 +268,37 @@ __global__ void __launch_bounds__(256) dfire_score_kernel(ScoreLaunch L) {
 }  // namespace sd
 
 #include "sd_score_mixed.cuh"
+#include "sd_score_ring.cuh"
 
 namespace sd {
+
+// compiled variants of the mixed DFIRE kernel (kernel, warps per CTA, minimum resident CTAs per
+// SM); the host autotuner times them on the context's own poses and keeps the fastest
+struct MixedVariant {
+  const void* fn;
+  int warps;
+  int min_blocks;
+};
+static const MixedVariant kMixedVariants[] = {
+    {(const void*)dfire_score_mixed_kernel<4, 4, false>, 4, 4},
+    {(const void*)dfire_score_mixed_kernel<4, 5, false>, 4, 5},
+    {(const void*)dfire_score_mixed_kernel<8, 2, false>, 8, 2},
+    {(const void*)dfire_score_mixed_kernel<4, 4, true>, 4, 4},
+    {(const void*)dfire_score_mixed_kernel<4, 5, true>, 4, 5},
+    {(const void*)dfire_score_mixed_kernel<8, 2, true>, 8, 2},
+    {(const void*)dfire_score_ring_kernel<4, 5, true, true>, 4, 5},
+    {(const void*)dfire_score_ring_kernel<4, 4, true, true>, 4, 4},
+    {(const void*)dfire_score_ring_kernel<8, 3, true, true>, 8, 3},
+    {(const void*)dfire_score_ring_kernel<4, 5, true, false>, 4, 5},
+    {(const void*)dfire_score_ring_kernel<4, 4, true, false>, 4, 4},
+    {(const void*)dfire_score_ring_kernel<8, 3, true, false>, 8, 3},
+    {(const void*)dfire_score_ring_kernel<4, 5, false, true>, 4, 5},
+    {(const void*)dfire_score_ring_kernel<4, 5, false, false>, 4, 5},
+};
+constexpr int kNumMixedVariants = sizeof(kMixedVariants) / sizeof(kMixedVariants[0]);
+static_assert(kNumMixedVariants <= SD_MAX_VARIANTS, "variant table");
+
+static const MixedVariant& mixed_variant(int v) { return kMixedVariants[v < 0 || v >= kNumMixedVariants ? 0 : v]; }
 
 size_t score_smem_bytes(int precision, int scoring, int max_nr, int max_nl) {
   if (scoring == SD_SCORING_PYDOCK) return pydock_smem_bytes(precision, false, max_nl, max_nr);
@@ -283,8 +312,8 @@ size_t score_smem_bytes(int precision, int scoring, int max_nr, int max_nl) {
 }
 
 int mixed_variant_count() { return kNumMixedVariants; }
-int mixed_variant_warps(int v) { return kMixedVariants[v < 0 || v >= kNumMixedVariants ? 0 : v].warps; }
-int mixed_variant_min_blocks(int v) { return kMixedVariants[v < 0 || v >= kNumMixedVariants ? 0 : v].min_blocks; }
+int mixed_variant_warps(int v) { return mixed_variant(v).warps; }
+int mixed_variant_min_blocks(int v) { return mixed_variant(v).min_blocks; }
 
 int score_threads_of(int precision, int scoring, int variant) {
   if (scoring == SD_SCORING_PYDOCK) return pydock_threads();
@@ -296,7 +325,7 @@ const void* score_kernel_ptr(int precision, int scoring, int variant) {
   switch (precision) {
     case SD_PREC_FP64_REF: return (const void*)dfire_score_kernel<SD_PREC_FP64_REF>;
     case SD_PREC_FP64: return (const void*)dfire_score_kernel<SD_PREC_FP64>;
-    default: return kMixedVariants[variant < 0 || variant >= kNumMixedVariants ? 0 : variant].fn;
+    default: return mixed_variant(variant).fn;
   }
 }
 
@@ -306,7 +335,12 @@ int score_launch(const ScoreLaunch& L, int precision, int scoring, int grid, int
   switch (precision) {
     case SD_PREC_FP64_REF: dfire_score_kernel<SD_PREC_FP64_REF><<<grid, threads, smem, st>>>(L); break;
     case SD_PREC_FP64: dfire_score_kernel<SD_PREC_FP64><<<grid, threads, smem, st>>>(L); break;
-    default: launch_mixed_variant(variant, L, grid, smem, st); break;
+    default: {
+      const MixedVariant& v = mixed_variant(variant);
+      void* args[] = {(void*)&L};
+      if (cudaLaunchKernel(v.fn, dim3(grid), dim3(v.warps * 32), args, smem, st) != cudaSuccess) return SD_ERR_CUDA;
+      break;
+    }
   }
   return cudaGetLastError() == cudaSuccess ? SD_OK : SD_ERR_CUDA;
 }

@@ -448,34 +448,4 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
   }
 }
 
-// compiled variants of the mixed kernel (warps per CTA, minimum resident CTAs per SM);
-// the host autotuner times them on the context's own poses and keeps the fastest
-struct MixedVariant {
-  const void* fn;
-  int warps;
-  int min_blocks;
-};
-static const MixedVariant kMixedVariants[] = {
-    {(const void*)dfire_score_mixed_kernel<4, 4, false>, 4, 4},
-    {(const void*)dfire_score_mixed_kernel<4, 5, false>, 4, 5},
-    {(const void*)dfire_score_mixed_kernel<8, 2, false>, 8, 2},
-    {(const void*)dfire_score_mixed_kernel<4, 4, true>, 4, 4},
-    {(const void*)dfire_score_mixed_kernel<4, 5, true>, 4, 5},
-    {(const void*)dfire_score_mixed_kernel<8, 2, true>, 8, 2},
-};
-constexpr int kNumMixedVariants = sizeof(kMixedVariants) / sizeof(kMixedVariants[0]);
-// variants 3..5 use the packed-FP16 pre-filter in stage 1
-inline bool mixed_variant_h16(int v) { return v >= 3; }
-
-inline void launch_mixed_variant(int v, const ScoreLaunch& L, int grid, size_t smem, cudaStream_t st) {
-  switch (v) {
-    case 1: dfire_score_mixed_kernel<4, 5, false><<<grid, 128, smem, st>>>(L); break;
-    case 2: dfire_score_mixed_kernel<8, 2, false><<<grid, 256, smem, st>>>(L); break;
-    case 3: dfire_score_mixed_kernel<4, 4, true><<<grid, 128, smem, st>>>(L); break;
-    case 4: dfire_score_mixed_kernel<4, 5, true><<<grid, 128, smem, st>>>(L); break;
-    case 5: dfire_score_mixed_kernel<8, 2, true><<<grid, 256, smem, st>>>(L); break;
-    default: dfire_score_mixed_kernel<4, 4, false><<<grid, 128, smem, st>>>(L); break;
-  }
-}
-
 }  // namespace sd

@@ -1,0 +1,427 @@
+// Mixed-precision DFIRE scoring, batch-buffered pair ring (included by sd_score.cu, after
+// sd_score_mixed.cuh, whose exact_pair_key it shares).
+//
+// Contract as sd_score_mixed.cuh: the energy of cdfire_calculate_dfire
+// (prepare_gso_tasks.cc:1522-1615) with every bin identical to the FP64 reference bin, FP64 sums
+// of FP64 table values in a free order.  Differences in how the work is organised:
+//  * candidates (ligand atoms within reach of a receptor tile) are staged 32 at a time into one
+//    of two per-warp batch buffers, in the bit order of the stage-1 mask (candidate 2i at
+//    position i, 2i+1 at position 16+i), so no mask reordering is needed;
+//  * stage 1 (kH16) tests a pair with the dot-product form of the distance in packed FP16,
+//    three HFMA2 per two candidates: s = r.l - |l|^2/2 >= (|r|^2 - thr)/2, on coordinates
+//    centred on the tile centre.  thr is set per tile from a proven bound on the FP16 error
+//    (below), so every pair whose FP32 d^2 is within the cutoff passes; tiles or poses whose
+//    magnitudes would make the bound loose pass every candidate, and stage 2 filters exactly;
+//  * a ring entry is 16 bits, (buffer, position, receptor lane); stage 2 reads the candidate and
+//    the receptor atom from two 512-byte buffers (mostly broadcast reads), recomputes the FP32
+//    d^2, takes the key from a fast reciprocal square root and compares d^2 with per-pose bin
+//    edges already widened by the FP32 error bound B (directed rounding), so a pair that is not
+//    near an edge has its FP64 bin proven; near pairs go to the exact FP64 transform;
+//  * a rejected or padding pair gathers a zero from the table's padding instead of branching,
+//    and the gathered values are added one drain later, so the gathers of one drain are in
+//    flight while the next drain's pairs are evaluated.
+//
+// FP16 bound (u = 2^-11, R >= |r - c| for the tile's atoms, Lb >= |l - c| for its candidates,
+// w = |l - c|^2 / 2):  |s_fp16 - (r.l - w)| <= u (2.001 R Lb + w) + 3u (1.002 R Lb + 1.001 w)
+// <= u (5.1 R Lb + 2.1 Lb^2) = Es, and the right-hand side rounds by at most u (R^2 + thr)/2 = Ea,
+// so thr = 225 + B + 2 Es + 2 Ea + 0.01 keeps every pair with FP32 d^2 <= 225 + B.
+#pragma once
+
+namespace sd {
+namespace {
+
+constexpr int kRingCap = 1088;  // < 64 left over + at most 32 x 32 from one batch
+constexpr int kZeroIdx = SD_TABLE_SIZE + 8;  // a zero in the table padding
+
+// exact_pair_key (sd_score_mixed.cuh) inlined: measured fewer spills here than the call
+__device__ __forceinline__ int exact_pair_key_inline(const DevComplex* C, int nslots, const double* pose,
+                                                     const double* q, const double* qi, const double* T, int slot,
+                                                     int j, int* edge) {
+  double rx, ry, rz, lx, ly, lz;
+  receptor_exact(*C, nslots, slot, pose, rx, ry, rz);
+  ligand_exact(*C, j, pose, q, qi, lx, ly, lz);
+  const double dx = rx - lx, dy = ry - ly, dz = rz - lz;
+  const double e2 = dx * dx + dy * dy + dz * dz;
+  *edge = 0;
+  if (!(e2 <= SD_CUTOFF2)) return -1;
+  if (e2 == 0.0) {
+    *edge = 1;
+    return 0;
+  }
+  const int key = exact_key_m(e2, T);
+  if (key == 29) *edge = 2;
+  return key;
+}
+
+struct __align__(16) RingBufs {
+  float4 candf[64];          // [buffer][position]: FP32 ligand atom centred on t, col bits
+  __half candh[16][8];       // position pair i: {x(2i), x(2i+1), y.., y.., z.., z.., -w.., -w..}
+  float4 rec[32];            // receptor atom of each lane centred on t, row bits
+  int cslot[64];             // [buffer][position]: ligand chunk slot (exact fallback only)
+  int pend[64];              // pending candidate ligand slots
+  unsigned short ring[kRingCap];  // (buffer << 10) | (position << 5) | lane
+};
+
+}  // namespace
+
+// kDual: stage 2 takes 64 ring entries per round, two per lane (else 32, one per lane)
+template <int kWarps, int kMinBlocks, bool kH16, bool kDual>
+__global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_ring_kernel(ScoreLaunch L) {
+  constexpr int kG = kDual ? 64 : 32;  // entries per stage-2 round
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ RingBufs wb[kWarps];
+  __shared__ double sh_pose[7 + 2 * SD_MAX_MODES];
+  __shared__ double sh_q[4], sh_qi[4];
+  __shared__ double sh_T[32];
+  __shared__ float4 sh_key4[32];  // per pose: {lower edge + B (up), upper edge - B (down), bin bits, -}
+  __shared__ double sh_red[kWarps];
+  __shared__ int sh_item, sh_ntile, sh_next;
+  __shared__ float sh_bound[4];
+  __shared__ float sh_rot[9];
+  __shared__ unsigned long long sh_cnt[5];  // fallback, d2 == 0, d2 == 225, pairs, evaluations
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid < 32) sh_T[tid] = c_T[tid];
+  if (tid < 5) sh_cnt[tid] = 0;
+  StepCtl* ctl = L.ctl;
+  const int parity = ctl->parity;
+  const int count = ctl->count[parity];
+  const int* work = L.work[parity];
+  unsigned n_done = 0;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  RingBufs& W = wb[warp];
+
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) sh_item = atomicAdd(&ctl->grab[parity], 1);
+    __syncthreads();
+    const int item = sh_item;
+    if (item >= count) break;
+    const int w = work[item];
+    const int ci = wi_complex(w), p = wi_local(w);
+    const DevComplex& C = L.cplx[ci];
+    const int nslots = nslots_of(C), pl = C.pl, nlc = C.nlchunks;
+    const double* pose_g = C.pos + (size_t)p * pl;
+    if (tid < pl) sh_pose[tid] = pose_g[tid];
+    __syncthreads();
+    if (tid == 0) {
+      for (int k = 0; k < 4; ++k) sh_q[k] = sh_pose[3 + k];
+      quat_inverse(sh_q, sh_qi);
+      float dR = 0.f, dL = 0.f;
+      for (int m = 0; m < C.nmr; ++m) dR += fabsf((float)sh_pose[7 + m]) * C.mnorm_r[m];
+      for (int m = 0; m < C.nml; ++m) dL += fabsf((float)sh_pose[7 + C.nmr + m]) * C.mnorm_l[m];
+      dR = dR * 1.0001f + 1e-4f;
+      dL = dL * 1.0001f + 1e-4f;
+      sh_bound[0] = dR;
+      sh_bound[1] = dL;
+      // bound of |FP32 d2 - FP64 d2| for pairs within 15.1 A (coordinates centred on t)
+      const float RL = C.lig_radius + dL;
+      const float u32 = 5.9604645e-8f;
+      sh_bound[2] = 2.0f * (2.02f * u32 * (26.2f * (2.0f * RL + 15.1f) + 228.0f) + 3.0f * u32 * 228.0f) + 1e-6f;
+      const double n = sqrt(sh_q[0] * sh_q[0] + sh_q[1] * sh_q[1] + sh_q[2] * sh_q[2] + sh_q[3] * sh_q[3]);
+      const float w0 = (float)(sh_q[0] / n), x = (float)(sh_q[1] / n), y = (float)(sh_q[2] / n),
+                  z = (float)(sh_q[3] / n);
+      sh_rot[0] = 1 - 2 * (y * y + z * z);
+      sh_rot[1] = 2 * (x * y - w0 * z);
+      sh_rot[2] = 2 * (x * z + w0 * y);
+      sh_rot[3] = 2 * (x * y + w0 * z);
+      sh_rot[4] = 1 - 2 * (x * x + z * z);
+      sh_rot[5] = 2 * (y * z - w0 * x);
+      sh_rot[6] = 2 * (x * z - w0 * y);
+      sh_rot[7] = 2 * (y * z + w0 * x);
+      sh_rot[8] = 1 - 2 * (x * x + y * y);
+      // ligand reference point (prepare_gso_tasks.cc:460, :513, :524-526)
+      double rx = C.lig_ref[0], ry = C.lig_ref[1], rz = C.lig_ref[2];
+      quat_rotate(sh_q, sh_qi, rx, ry, rz);
+      double* ref = C.ref + (size_t)p * 3;
+      ref[0] = rx + sh_pose[0];
+      ref[1] = ry + sh_pose[1];
+      ref[2] = rz + sh_pose[2];
+      sh_ntile = 0;
+      sh_next = 0;
+    }
+    __syncthreads();
+    const double tx = sh_pose[0], ty = sh_pose[1], tz = sh_pose[2];
+    const float dR = sh_bound[0], dL = sh_bound[1], B = sh_bound[2];
+    if (tid < 32) {
+      // bin edges of key tid widened by B; a pair strictly inside them has its FP64 bin proven
+      const int k = tid < 30 ? tid : 29;
+      sh_key4[tid] = make_float4(__fadd_ru(c_Tf[k], B), __fsub_rd(c_Tf[k + 1], B), __int_as_float(c_binlut[k]), 0.f);
+    }
+    float4* ligS = reinterpret_cast<float4*>(smem);  // [nlc*32] centred on t, col bits
+    float4* chS = ligS + (size_t)nlc * SD_TILE;      // [nlc] centre + radius
+    int* tlist = reinterpret_cast<int*>(chS + nlc);  // [ntiles] tiles within reach
+    for (int s = tid; s < nlc * SD_TILE; s += blockDim.x) {
+      const int j = C.l_perm[s];
+      if (j >= 0) {
+        double x, y, z;
+        ligand_exact(C, j, sh_pose, sh_q, sh_qi, x, y, z);
+        ligS[s] = make_float4((float)(x - tx), (float)(y - ty), (float)(z - tz), __int_as_float(C.l_col[j]));
+      } else {
+        ligS[s] = make_float4(1e18f, 1e18f, 1e18f, __int_as_float(0));
+      }
+    }
+    for (int c = tid; c < nlc; c += blockDim.x) {
+      const float4 cc = C.l_chunk[c];
+      const float X = sh_rot[0] * cc.x + sh_rot[1] * cc.y + sh_rot[2] * cc.z;
+      const float Y = sh_rot[3] * cc.x + sh_rot[4] * cc.y + sh_rot[5] * cc.z;
+      const float Z = sh_rot[6] * cc.x + sh_rot[7] * cc.y + sh_rot[8] * cc.z;
+      chS[c] = make_float4(X, Y, Z, cc.w + dL);
+    }
+    const float lig_reach = C.lig_radius + dL;
+    for (int k = tid; k < C.ntiles; k += blockDim.x) {
+      const float4 tile = C.r_tile[k];
+      const float cx = (float)((double)tile.x - tx), cy = (float)((double)tile.y - ty),
+                  cz = (float)((double)tile.z - tz);
+      const float reach = 15.0f + dR + SD_CULL_MARGIN + tile.w + lig_reach;
+      if (cx * cx + cy * cy + cz * cz <= reach * reach) tlist[atomicAdd(&sh_ntile, 1)] = k;
+    }
+    __syncthreads();
+    const int ntile = sh_ntile;
+    const float cut2 = 225.0f + B;
+    double acc = 0.0;               // per-lane FP64 sum of table values
+    double pv0 = 0.0, pv1 = 0.0;    // values gathered by the previous drain, added by the next
+    unsigned npairs = 0, nevals = 0;
+
+    for (;;) {
+      int ti = 0;
+      if (lane == 0) ti = atomicAdd(&sh_next, 1);
+      ti = __shfl_sync(0xffffffffu, ti, 0);
+      if (ti >= ntile) break;
+      const int k = tlist[ti];
+      const float4 tile = C.r_tile[k];
+      const float cx = (float)((double)tile.x - tx), cy = (float)((double)tile.y - ty),
+                  cz = (float)((double)tile.z - tz);
+      const float reach = 15.0f + dR + SD_CULL_MARGIN + tile.w;
+      const float reach2 = reach * reach;
+      const int slot = k * SD_TILE + lane;
+      const bool active = C.r_orig[slot] >= 0;
+      float fx = 1e18f, fy = 1e18f, fz = 1e18f;
+      int row = 0;
+      if (active) {
+        double rx, ry, rz;
+        receptor_exact(C, nslots, slot, sh_pose, rx, ry, rz);
+        fx = (float)(rx - tx);
+        fy = (float)(ry - ty);
+        fz = (float)(rz - tz);
+        row = C.r_row[slot];
+      }
+      W.rec[lane] = make_float4(fx, fy, fz, __int_as_float(row));
+      const unsigned act_mask = __ballot_sync(0xffffffffu, active);
+      const int nact = __popc(act_mask);
+      // stage-1 constants of this lane
+      __half2 rx2, ry2, rz2, a2;
+      const float R = tile.w + dR + SD_CULL_MARGIN, Lb = reach + 0.01f;
+      const bool tight = R <= 40.0f && Lb <= 80.0f;  // warp-uniform
+      if (kH16) {
+        const float u16 = 4.8828125e-4f;
+        const float Es = u16 * (5.1f * R * Lb + 2.1f * Lb * Lb);
+        const float thr0 = 225.0f + B + 1e-3f + 2.0f * Es;
+        const float thr = thr0 + u16 * (R * R + thr0 + 10.0f) + 2e-4f + 0.01f;
+        const float ux = fx - cx, uy = fy - cy, uz = fz - cz;
+        const float a = 0.5f * (ux * ux + uy * uy + uz * uz) - 0.5f * thr;
+        const bool use = active && tight;
+        rx2 = __float2half2_rn(use ? ux : 0.f);
+        ry2 = __float2half2_rn(use ? uy : 0.f);
+        rz2 = __float2half2_rn(use ? uz : 0.f);
+        // loose tile: every candidate passes (s = 0 > -65504); inactive lane: none does
+        a2 = __float2half2_rn(!active ? 65504.f : (tight ? a : -65504.f));
+      }
+      int ncand = 0, head = 0, par = 0, oldL = 0;  // ring holds entries [0, head)
+      int cb = 0;
+      unsigned cm = 0;
+
+      for (;;) {
+        // collect candidates until a batch is full or the ligand is exhausted
+        while (ncand < 32) {
+          if (cm == 0) {
+            if (cb >= nlc) break;
+            const int c = cb + lane;
+            bool cnear = false;
+            if (c < nlc) {
+              const float4 ch = chS[c];
+              const float ex = ch.x - cx, ey = ch.y - cy, ez = ch.z - cz, r = reach + ch.w;
+              cnear = ex * ex + ey * ey + ez * ez <= r * r;
+            }
+            cm = __ballot_sync(0xffffffffu, cnear);
+            cb += 32;
+            continue;
+          }
+          const int sb = (cb - 32 + __ffs(cm) - 1) * SD_TILE;
+          cm &= cm - 1;
+          const float4 la = ligS[sb + lane];
+          const float ax = la.x - cx, ay = la.y - cy, az = la.z - cz;
+          const bool cand = ax * ax + ay * ay + az * az <= reach2;
+          const unsigned am = __ballot_sync(0xffffffffu, cand);
+          if (cand) W.pend[ncand + __popc(am & lt_mask)] = sb + lane;
+          ncand += __popc(am);
+        }
+        const bool exhausted = cm == 0 && cb >= nlc;
+        if (ncand == 0 && head == 0) break;
+        const int nb = min(ncand, 32);
+        const bool final_batch = exhausted && ncand <= 32;
+        if (nb > 0) {
+          // stage the batch into buffer par, in mask bit order
+          __syncwarp();
+          const int pos = (lane >> 1) | ((lane & 1) << 4);
+          float4 l4 = make_float4(-1e18f, -1e18f, -1e18f, 0.f);
+          int s = 0;
+          if (lane < nb) {
+            s = W.pend[lane];
+            l4 = ligS[s];
+          }
+          W.candf[par * 32 + pos] = l4;
+          W.cslot[par * 32 + pos] = s;
+          if (kH16) {
+            // unused place: s = -60000, never in range; loose tile: every place passes
+            float lx = 0.f, ly = 0.f, lz = 0.f, nw = tight ? -60000.f : 0.f;
+            if (lane < nb && tight) {
+              lx = l4.x - cx;
+              ly = l4.y - cy;
+              lz = l4.z - cz;
+              nw = fmaxf(-0.5f * (lx * lx + ly * ly + lz * lz), -60000.f);
+            }
+            __half* q = W.candh[lane >> 1];
+            q[0 + (lane & 1)] = __float2half_rn(lx);
+            q[2 + (lane & 1)] = __float2half_rn(ly);
+            q[4 + (lane & 1)] = __float2half_rn(lz);
+            q[6 + (lane & 1)] = __float2half_rn(nw);
+          }
+          __syncwarp();
+          // stage 1: bit b of m <=> (this lane's receptor atom, candidate at position b) in range
+          unsigned M = 0;
+          if (kH16) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+              const uint4 qq = *reinterpret_cast<const uint4*>(W.candh[i]);
+              __half2 sv = __hfma2(rx2, *reinterpret_cast<const __half2*>(&qq.x), *reinterpret_cast<const __half2*>(&qq.w));
+              sv = __hfma2(ry2, *reinterpret_cast<const __half2*>(&qq.y), sv);
+              sv = __hfma2(rz2, *reinterpret_cast<const __half2*>(&qq.z), sv);
+              M |= __hge2_mask(sv, a2) & (0x00010001u << i);
+            }
+          } else {
+#pragma unroll
+            for (int b = 0; b < 32; ++b) {
+              const float4 l = W.candf[par * 32 + b];
+              const float ex = fx - l.x, ey = fy - l.y, ez = fz - l.z;
+              const float d2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
+              M |= (d2 <= cut2 ? 1u : 0u) << b;
+            }
+          }
+          const unsigned lo = (1u << ((nb + 1) >> 1)) - 1u, hi = (1u << (nb >> 1)) - 1u;
+          unsigned m = M & (lo | (hi << 16)) & (active ? 0xffffffffu : 0u);
+          nevals += lane == 0 ? (unsigned)(nb * nact) : 0u;
+          // append this lane's pairs to the ring
+          const int cnt = __popc(m);
+          int incl = cnt;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+          }
+          const int total = __shfl_sync(0xffffffffu, incl, 31);
+          int at = head + incl - cnt;
+          const unsigned tag = ((unsigned)par << 10) | (unsigned)lane;
+          while (m) {
+            const int b = 31 - __clz(m);
+            m ^= 1u << b;
+            W.ring[at++] = (unsigned short)(tag | ((unsigned)b << 5));
+          }
+          head += total;
+          // keep the candidates beyond the first 32
+          const int rest = ncand - nb;
+          int carry = 0;
+          if (lane < rest) carry = W.pend[32 + lane];
+          __syncwarp();
+          if (lane < rest) W.pend[lane] = carry;
+          ncand = rest;
+          par ^= 1;
+        }
+        __syncwarp();
+        // stage 2: drain whole rounds of kG; everything at the end of the tile, or when entries
+        // of the previous batch would otherwise outlive its buffer
+        const int upto = (final_batch || (oldL > 0 && head < kG)) ? head : (head & ~(kG - 1));
+        auto pair = [&](int t0, int h, int n) -> double {
+          const unsigned e = W.ring[t0 + h * 32 + lane];
+          const int cix = (int)(e >> 5) & 63, rl = (int)e & 31;
+          const float4 lf = W.candf[cix];
+          const float4 rr = W.rec[rl];
+          const float ex = rr.x - lf.x, ey = rr.y - lf.y, ez = rr.z - lf.z;
+          const float d2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
+          bool ok = (h * 32 + lane < n) && d2 <= cut2;
+          // key estimate; d2 == 0 gives NaN -> 0 and lies within B of edge 0 (exact path)
+          const float r = d2 * rsqrtf(d2);
+          const int key = (int)fmaf(r, 2.0f, -1.0f) & 31;
+          const float4 kk = sh_key4[key];
+          int idx = __float_as_int(rr.w) + __float_as_int(lf.w) + __float_as_int(kk.z);
+          if (ok && (d2 <= kk.x || d2 >= kk.y)) {
+            atomicAdd(&sh_cnt[0], 1ull);
+            int edge;
+            const int kx = exact_pair_key_inline(&C, nslots, sh_pose, sh_q, sh_qi, sh_T, k * SD_TILE + rl,
+                                          C.l_perm[W.cslot[cix]], &edge);
+            if (kx < 0) {
+              ok = false;
+            } else {
+              idx = __float_as_int(rr.w) + __float_as_int(lf.w) + c_binlut[kx];
+              if (edge) atomicAdd(&sh_cnt[edge], 1ull);
+            }
+          }
+          npairs += ok ? 1u : 0u;
+          return __ldg(L.table64 + (ok ? idx : kZeroIdx));
+        };
+        for (int t0 = 0; t0 < upto; t0 += kG) {
+          acc += pv0;
+          const int n = min(kG, upto - t0);
+          pv0 = pair(t0, 0, n);
+          if (kDual) {
+            acc += pv1;
+            pv1 = pair(t0, 1, n);
+          }
+        }
+        // move the leftover (< kG) entries to the front
+        const int left = head - upto;
+        unsigned short e0 = 0, e1 = 0;
+        if (lane < left) e0 = W.ring[upto + lane];
+        if (lane + 32 < left) e1 = W.ring[upto + 32 + lane];
+        __syncwarp();
+        if (lane < left) W.ring[lane] = e0;
+        if (lane + 32 < left) W.ring[lane + 32] = e1;
+        head = left;
+        oldL = left;
+        if (final_batch) break;
+      }
+      __syncwarp();
+    }
+    acc += pv0;
+    acc += pv1;
+    // counters, then the FP64 block reduction of the per-lane sums
+    const unsigned wp = __reduce_add_sync(0xffffffffu, npairs);
+    if (lane == 0) {
+      if (wp) atomicAdd(&sh_cnt[3], (unsigned long long)wp);
+      if (nevals) atomicAdd(&sh_cnt[4], (unsigned long long)nevals);
+    }
+    double v = acc;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) sh_red[warp] = v;
+    __syncthreads();
+    if (tid == 0) {
+      double E = 0.0;
+      for (int i = 0; i < kWarps; ++i) E += sh_red[i];
+      const double score = ((E)*0.0157 - 4.7) * -1;
+      C.scoring[p] = score;
+      if (L.energy_out) L.energy_out[p] = E;
+      ++n_done;
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    if (n_done) atomicAdd(&ctl->stats[ST_SCORED], (unsigned long long)n_done);
+    if (sh_cnt[0]) atomicAdd(&ctl->stats[ST_FALLBACK], sh_cnt[0]);
+    if (sh_cnt[1]) atomicAdd(&ctl->stats[ST_D2ZERO], sh_cnt[1]);
+    if (sh_cnt[2]) atomicAdd(&ctl->stats[ST_D2CUT], sh_cnt[2]);
+    if (sh_cnt[3]) atomicAdd(&ctl->stats[ST_PAIRS], sh_cnt[3]);
+    if (sh_cnt[4]) atomicAdd(&ctl->stats[ST_EVALS], sh_cnt[4]);
+  }
+}
+
+}  // namespace sd

@@ -157,7 +157,7 @@ def test_multi_complex_batch_mixed_scores(tables):
         assert dk.stats()["guard_errors"] == 0
 
 
-@pytest.mark.parametrize("variant", range(6))
+@pytest.mark.parametrize("variant", range(sd.mixed_variant_count()))
 def test_every_mixed_kernel_variant(variant, c0, tables, monkeypatch):
     """Each compiled variant of the mixed kernel (the autotuner may pick any) scores the first
     step's poses within 1e-5 of the FP64 oracle, with no index guard firing."""
