@@ -346,9 +346,29 @@ int setup_complex(sd_ctx* c, const sd_complex_desc& d, ComplexHost& h, int gbase
       }
       lch[t] = make_float4(cf[0], cf[1], cf[2], round_up_f(rad * (1 + 1e-6) + 1e-4));
     }
+    const size_t nls = lslots.size();
+    std::vector<double> cxyz(nls * 3, 0.0), cmodes((size_t)std::max(1, D.nml) * nls * 3, 0.0);
+    std::vector<int> cmask(nls, 0), ccol(nls, 0);
+    for (size_t s = 0; s < nls; ++s) {
+      const int j = lslots[s];
+      if (j < 0) continue;
+      for (int k = 0; k < 3; ++k) cxyz[s * 3 + k] = d.lig_xyz[(size_t)j * 3 + k];
+      for (int m = 0; m < D.nml; ++m)
+        for (int k = 0; k < 3; ++k) cmodes[((size_t)m * nls + s) * 3 + k] = d.lig_modes[((size_t)m * d.n_lig + j) * 3 + k];
+      cmask[s] = d.lig_mask[j];
+      ccol[s] = d.lig_dfire_type[j] * SD_DFIRE_BINS;
+    }
+    double lc[3] = {0, 0, 0};
+    for (int j = 0; j < d.n_lig; ++j)
+      for (int k = 0; k < 3; ++k) lc[k] += d.lig_xyz[(size_t)j * 3 + k];
+    for (int k = 0; k < 3; ++k) D.lig_ctr[k] = (float)(lc[k] / std::max(1, d.n_lig));
     int rc2;
     if ((rc2 = upload(c, h, lslots.data(), lslots.size(), &D.l_perm))) return rc2;
     if ((rc2 = upload(c, h, lch.data(), lch.size(), &D.l_chunk))) return rc2;
+    if ((rc2 = upload(c, h, cxyz.data(), cxyz.size(), &D.lc_xyz))) return rc2;
+    if ((rc2 = upload(c, h, cmodes.data(), cmodes.size(), &D.lc_modes))) return rc2;
+    if ((rc2 = upload(c, h, cmask.data(), cmask.size(), &D.lc_mask))) return rc2;
+    if ((rc2 = upload(c, h, ccol.data(), ccol.size(), &D.lc_col))) return rc2;
   }
   std::vector<int> lcol(d.n_lig), llj(d.n_lig, 0);
   std::vector<float> lq(d.n_lig, 0.f);

@@ -59,6 +59,12 @@ struct DevComplex {
   int nlchunks;
   const int* l_perm;       // [nlchunks*32] chunk slot -> original ligand index, or -1
   const float4* l_chunk;   // [nlchunks] centre (ligand frame) + radius
+  // the ligand again in chunk-slot order (coalesced reads in the mixed kernels; padding slots 0)
+  const double* lc_xyz;    // [nlchunks*32][3]
+  const double* lc_modes;  // [nml][nlchunks*32][3]
+  const int* lc_mask;      // [nlchunks*32]
+  const int* lc_col;       // [nlchunks*32]
+  float lig_ctr[3];        // ligand centroid (ligand frame)
   float mnorm_r[SD_MAX_MODES], mnorm_l[SD_MAX_MODES];  // max per-atom mode norm (rounded up)
   float lig_radius;        // max |l0_j| (rounded up)
   float rec_span;          // max |r0_i - origin| (rounded up)

@@ -71,6 +71,29 @@ __device__ __forceinline__ void ligand_exact(const DevComplex& C, int j, const d
   z += pose[2];
 }
 
+// ligand atom in chunk slot s (chunk-ordered copies, same arithmetic as ligand_exact)
+__device__ __forceinline__ void ligand_exact_chunk(const DevComplex& C, int s, const double* pose, const double* q,
+                                                   const double* qi, double& x, double& y, double& z) {
+  const int nls = C.nlchunks * SD_TILE;
+  x = C.lc_xyz[s * 3];
+  y = C.lc_xyz[s * 3 + 1];
+  z = C.lc_xyz[s * 3 + 2];
+  const int mk = C.lc_mask[s];
+  for (int m = 0; m < C.nml; ++m) {
+    const double e = pose[7 + C.nmr + m];
+    const double* M = C.lc_modes + ((size_t)m * nls + s) * 3;
+    if (mk == 1) {
+      x += M[0] * e;
+      y += M[1] * e;
+      z += M[2] * e;
+    }
+  }
+  quat_rotate(q, qi, x, y, z);
+  x += pose[0];
+  y += pose[1];
+  z += pose[2];
+}
+
 __device__ __forceinline__ int nslots_of(const DevComplex& C) { return C.ntiles * SD_TILE; }
 
 }  // namespace sd

@@ -280,20 +280,15 @@ struct MixedVariant {
   int min_blocks;
 };
 static const MixedVariant kMixedVariants[] = {
-    {(const void*)dfire_score_mixed_kernel<4, 4, false>, 4, 4},
-    {(const void*)dfire_score_mixed_kernel<4, 5, false>, 4, 5},
-    {(const void*)dfire_score_mixed_kernel<8, 2, false>, 8, 2},
     {(const void*)dfire_score_mixed_kernel<4, 4, true>, 4, 4},
-    {(const void*)dfire_score_mixed_kernel<4, 5, true>, 4, 5},
-    {(const void*)dfire_score_mixed_kernel<8, 2, true>, 8, 2},
-    {(const void*)dfire_score_ring_kernel<4, 5, true, true>, 4, 5},
-    {(const void*)dfire_score_ring_kernel<4, 4, true, true>, 4, 4},
-    {(const void*)dfire_score_ring_kernel<8, 3, true, true>, 8, 3},
-    {(const void*)dfire_score_ring_kernel<4, 5, true, false>, 4, 5},
-    {(const void*)dfire_score_ring_kernel<4, 4, true, false>, 4, 4},
-    {(const void*)dfire_score_ring_kernel<8, 3, true, false>, 8, 3},
-    {(const void*)dfire_score_ring_kernel<4, 5, false, true>, 4, 5},
-    {(const void*)dfire_score_ring_kernel<4, 5, false, false>, 4, 5},
+    {(const void*)dfire_score_ring_kernel<8, 3, true, true, false>, 8, 3},
+    {(const void*)dfire_score_ring_kernel<4, 5, true, true, false>, 4, 5},
+    {(const void*)dfire_score_ring_kernel<8, 3, true, true, true>, 8, 3},
+    {(const void*)dfire_score_ring_kernel<4, 5, true, true, true>, 4, 5},
+    {(const void*)dfire_score_ring_kernel<4, 4, true, true, true>, 4, 4},
+    {(const void*)dfire_score_ring_kernel<8, 3, true, false, true>, 8, 3},
+    {(const void*)dfire_score_ring_kernel<8, 2, true, true, true>, 8, 2},
+    {(const void*)dfire_score_ring_kernel<4, 5, false, true, true>, 4, 5},
 };
 constexpr int kNumMixedVariants = sizeof(kMixedVariants) / sizeof(kMixedVariants[0]);
 static_assert(kNumMixedVariants <= SD_MAX_VARIANTS, "variant table");
@@ -305,7 +300,7 @@ size_t score_smem_bytes(int precision, int scoring, int max_nr, int max_nl) {
   if (precision == SD_PREC_MIXED) {
     const size_t nlc = (size_t)(max_nl + SD_TILE - 1) / SD_TILE;
     const size_t ntiles = (size_t)(max_nr + SD_TILE - 1) / SD_TILE;
-    return (size_t)16 * (nlc * SD_TILE + nlc) + 4 * ntiles;
+    return (size_t)16 * (nlc * SD_TILE + nlc) + 4 * (3 * ntiles + nlc);
   }
   return (size_t)16 * ((max_nl + 1) & ~1) + (size_t)32 * max_nl + (size_t)8 * max_nr +
          (size_t)4 * ((max_nr + SD_TILE - 1) / SD_TILE);

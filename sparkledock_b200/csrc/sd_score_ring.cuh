@@ -64,16 +64,22 @@ struct __align__(16) RingBufs {
 
 }  // namespace
 
-// kDual: stage 2 takes 64 ring entries per round, two per lane (else 32, one per lane)
-template <int kWarps, int kMinBlocks, bool kH16, bool kDual>
+// kDual: stage 2 takes 64 ring entries per round, two per lane (else 32, one per lane).
+// kSoA: candidate buffers as separate x / y / z / col arrays (conflict-free 4-byte reads in stage
+// 2) instead of one float4 per candidate.
+template <int kWarps, int kMinBlocks, bool kH16, bool kDual, bool kSoA>
 __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_ring_kernel(ScoreLaunch L) {
   constexpr int kG = kDual ? 64 : 32;  // entries per stage-2 round
+  constexpr int kSortMax = 512;        // near tiles ordered largest-first up to this many
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ RingBufs wb[kWarps];
   __shared__ double sh_pose[7 + 2 * SD_MAX_MODES];
   __shared__ double sh_q[4], sh_qi[4];
   __shared__ double sh_T[32];
-  __shared__ float4 sh_key4[32];  // per pose: {lower edge + B (up), upper edge - B (down), bin bits, -}
+  // per pose and key k: lower edge + B (rounded up), upper edge - B (rounded down), bin
+  __shared__ float sh_klo[32], sh_khi[32];
+  __shared__ int sh_kbin[32];
+  __shared__ float sh_gc[3];      // ligand centroid, rotated (centred on t)
   __shared__ double sh_red[kWarps];
   __shared__ int sh_item, sh_ntile, sh_next;
   __shared__ float sh_bound[4];
@@ -130,6 +136,8 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_ring_kern
       sh_rot[6] = 2 * (x * z - w0 * y);
       sh_rot[7] = 2 * (y * z + w0 * x);
       sh_rot[8] = 1 - 2 * (x * x + y * y);
+      for (int a = 0; a < 3; ++a)
+        sh_gc[a] = sh_rot[3 * a] * C.lig_ctr[0] + sh_rot[3 * a + 1] * C.lig_ctr[1] + sh_rot[3 * a + 2] * C.lig_ctr[2];
       // ligand reference point (prepare_gso_tasks.cc:460, :513, :524-526)
       double rx = C.lig_ref[0], ry = C.lig_ref[1], rz = C.lig_ref[2];
       quat_rotate(sh_q, sh_qi, rx, ry, rz);
@@ -146,30 +154,27 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_ring_kern
     if (tid < 32) {
       // bin edges of key tid widened by B; a pair strictly inside them has its FP64 bin proven
       const int k = tid < 30 ? tid : 29;
-      sh_key4[tid] = make_float4(__fadd_ru(c_Tf[k], B), __fsub_rd(c_Tf[k + 1], B), __int_as_float(c_binlut[k]), 0.f);
+      sh_klo[tid] = __fadd_ru(c_Tf[k], B);
+      sh_khi[tid] = __fsub_rd(c_Tf[k + 1], B);
+      sh_kbin[tid] = c_binlut[k];
     }
-    float4* ligS = reinterpret_cast<float4*>(smem);  // [nlc*32] centred on t, col bits
-    float4* chS = ligS + (size_t)nlc * SD_TILE;      // [nlc] centre + radius
+    const int nls = nlc * SD_TILE, ntiles = C.ntiles;
+    float4* ligS = reinterpret_cast<float4*>(smem);  // [nls] centred on t, col bits
+    float4* chS = ligS + nls;                        // [nlc] centre + radius
     int* tlist = reinterpret_cast<int*>(chS + nlc);  // [ntiles] tiles within reach
-    for (int s = tid; s < nlc * SD_TILE; s += blockDim.x) {
-      const int j = C.l_perm[s];
-      if (j >= 0) {
-        double x, y, z;
-        ligand_exact(C, j, sh_pose, sh_q, sh_qi, x, y, z);
-        ligS[s] = make_float4((float)(x - tx), (float)(y - ty), (float)(z - tz), __int_as_float(C.l_col[j]));
-      } else {
-        ligS[s] = make_float4(1e18f, 1e18f, 1e18f, __int_as_float(0));
-      }
-    }
+    int* tord = tlist + ntiles;                      // [ntiles] the same, largest first
+    float* tdist = reinterpret_cast<float*>(tord + ntiles);  // [ntiles]
+    int* cneed = reinterpret_cast<int*>(tdist + ntiles);     // [nlc] chunk within reach of a near tile
     for (int c = tid; c < nlc; c += blockDim.x) {
       const float4 cc = C.l_chunk[c];
       const float X = sh_rot[0] * cc.x + sh_rot[1] * cc.y + sh_rot[2] * cc.z;
       const float Y = sh_rot[3] * cc.x + sh_rot[4] * cc.y + sh_rot[5] * cc.z;
       const float Z = sh_rot[6] * cc.x + sh_rot[7] * cc.y + sh_rot[8] * cc.z;
       chS[c] = make_float4(X, Y, Z, cc.w + dL);
+      cneed[c] = 0;
     }
     const float lig_reach = C.lig_radius + dL;
-    for (int k = tid; k < C.ntiles; k += blockDim.x) {
+    for (int k = tid; k < ntiles; k += blockDim.x) {
       const float4 tile = C.r_tile[k];
       const float cx = (float)((double)tile.x - tx), cy = (float)((double)tile.y - ty),
                   cz = (float)((double)tile.z - tz);
@@ -178,6 +183,50 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_ring_kern
     }
     __syncthreads();
     const int ntile = sh_ntile;
+    const bool sorted = ntile <= kSortMax;
+    // distance of each near tile from the ligand centroid (closest tiles have the most pairs),
+    // and which ligand chunks any near tile can reach (the same test as the per-tile one below,
+    // with 0.01 A to spare, so a chunk that is not needed is never read)
+    for (int t = tid; t < ntile; t += blockDim.x) {
+      const float4 tile = C.r_tile[tlist[t]];
+      const float ex = (float)((double)tile.x - tx) - sh_gc[0], ey = (float)((double)tile.y - ty) - sh_gc[1],
+                  ez = (float)((double)tile.z - tz) - sh_gc[2];
+      tdist[t] = ex * ex + ey * ey + ez * ez;
+    }
+    for (int i = tid; i < ntile * nlc; i += blockDim.x) {
+      const int t = i / nlc, c = i - t * nlc;
+      const float4 tile = C.r_tile[tlist[t]];
+      const float cx = (float)((double)tile.x - tx), cy = (float)((double)tile.y - ty),
+                  cz = (float)((double)tile.z - tz);
+      const float4 ch = chS[c];
+      const float ex = ch.x - cx, ey = ch.y - cy, ez = ch.z - cz,
+                  r = (15.0f + dR + SD_CULL_MARGIN + tile.w) + ch.w + 0.01f;
+      if (ex * ex + ey * ey + ez * ez <= r * r) cneed[c] = 1;
+    }
+    __syncthreads();
+    if (sorted) {
+      for (int t = tid; t < ntile; t += blockDim.x) {
+        const float d = tdist[t];
+        int rank = 0;
+        for (int u = 0; u < ntile; ++u) {
+          const float e = tdist[u];
+          rank += (e < d || (e == d && u < t)) ? 1 : 0;
+        }
+        tord[rank] = tlist[t];
+      }
+    }
+    for (int s = tid; s < nls; s += blockDim.x) {
+      if (!cneed[s >> 5]) continue;
+      if (C.l_perm[s] >= 0) {
+        double x, y, z;
+        ligand_exact_chunk(C, s, sh_pose, sh_q, sh_qi, x, y, z);
+        ligS[s] = make_float4((float)(x - tx), (float)(y - ty), (float)(z - tz), __int_as_float(C.lc_col[s]));
+      } else {
+        ligS[s] = make_float4(1e18f, 1e18f, 1e18f, __int_as_float(0));
+      }
+    }
+    __syncthreads();
+    const int* tl = sorted ? tord : tlist;
     const float cut2 = 225.0f + B;
     double acc = 0.0;               // per-lane FP64 sum of table values
     double pv0 = 0.0, pv1 = 0.0;    // values gathered by the previous drain, added by the next
@@ -188,7 +237,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_ring_kern
       if (lane == 0) ti = atomicAdd(&sh_next, 1);
       ti = __shfl_sync(0xffffffffu, ti, 0);
       if (ti >= ntile) break;
-      const int k = tlist[ti];
+      const int k = tl[ti];
       const float4 tile = C.r_tile[k];
       const float cx = (float)((double)tile.x - tx), cy = (float)((double)tile.y - ty),
                   cz = (float)((double)tile.z - tz);
@@ -241,7 +290,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_ring_kern
             if (c < nlc) {
               const float4 ch = chS[c];
               const float ex = ch.x - cx, ey = ch.y - cy, ez = ch.z - cz, r = reach + ch.w;
-              cnear = ex * ex + ey * ey + ez * ez <= r * r;
+              cnear = ex * ex + ey * ey + ez * ez <= r * r;  // same expression as the cneed test
             }
             cm = __ballot_sync(0xffffffffu, cnear);
             cb += 32;
@@ -251,7 +300,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_ring_kern
           cm &= cm - 1;
           const float4 la = ligS[sb + lane];
           const float ax = la.x - cx, ay = la.y - cy, az = la.z - cz;
-          const bool cand = ax * ax + ay * ay + az * az <= reach2;
+          const bool cand = fmaf(az, az, fmaf(ay, ay, ax * ax)) <= reach2;
           const unsigned am = __ballot_sync(0xffffffffu, cand);
           if (cand) W.pend[ncand + __popc(am & lt_mask)] = sb + lane;
           ncand += __popc(am);
@@ -270,7 +319,15 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_ring_kern
             s = W.pend[lane];
             l4 = ligS[s];
           }
-          W.candf[par * 32 + pos] = l4;
+          if (kSoA) {
+            float* cf = reinterpret_cast<float*>(W.candf);
+            cf[par * 32 + pos] = l4.x;
+            cf[64 + par * 32 + pos] = l4.y;
+            cf[128 + par * 32 + pos] = l4.z;
+            cf[192 + par * 32 + pos] = l4.w;
+          } else {
+            W.candf[par * 32 + pos] = l4;
+          }
           W.cslot[par * 32 + pos] = s;
           if (kH16) {
             // unused place: s = -60000, never in range; loose tile: every place passes
@@ -302,7 +359,13 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_ring_kern
           } else {
 #pragma unroll
             for (int b = 0; b < 32; ++b) {
-              const float4 l = W.candf[par * 32 + b];
+              float4 l;
+              if (kSoA) {
+                const float* cf = reinterpret_cast<const float*>(W.candf);
+                l = make_float4(cf[par * 32 + b], cf[64 + par * 32 + b], cf[128 + par * 32 + b], 0.f);
+              } else {
+                l = W.candf[par * 32 + b];
+              }
               const float ex = fx - l.x, ey = fy - l.y, ez = fz - l.z;
               const float d2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
               M |= (d2 <= cut2 ? 1u : 0u) << b;
@@ -344,7 +407,13 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_ring_kern
         auto pair = [&](int t0, int h, int n) -> double {
           const unsigned e = W.ring[t0 + h * 32 + lane];
           const int cix = (int)(e >> 5) & 63, rl = (int)e & 31;
-          const float4 lf = W.candf[cix];
+          float4 lf;
+          if (kSoA) {
+            const float* cf = reinterpret_cast<const float*>(W.candf);
+            lf = make_float4(cf[cix], cf[64 + cix], cf[128 + cix], cf[192 + cix]);
+          } else {
+            lf = W.candf[cix];
+          }
           const float4 rr = W.rec[rl];
           const float ex = rr.x - lf.x, ey = rr.y - lf.y, ez = rr.z - lf.z;
           const float d2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
@@ -352,9 +421,8 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_ring_kern
           // key estimate; d2 == 0 gives NaN -> 0 and lies within B of edge 0 (exact path)
           const float r = d2 * rsqrtf(d2);
           const int key = (int)fmaf(r, 2.0f, -1.0f) & 31;
-          const float4 kk = sh_key4[key];
-          int idx = __float_as_int(rr.w) + __float_as_int(lf.w) + __float_as_int(kk.z);
-          if (ok && (d2 <= kk.x || d2 >= kk.y)) {
+          int idx = __float_as_int(rr.w) + __float_as_int(lf.w) + sh_kbin[key];
+          if (ok && (d2 <= sh_klo[key] || d2 >= sh_khi[key])) {
             atomicAdd(&sh_cnt[0], 1ull);
             int edge;
             const int kx = exact_pair_key_inline(&C, nslots, sh_pose, sh_q, sh_qi, sh_T, k * SD_TILE + rl,
