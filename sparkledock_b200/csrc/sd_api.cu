@@ -119,6 +119,7 @@ struct sd_ctx {
   DevComplex* d_cplx = nullptr;
   DevComplex* d_cplx_scratch = nullptr;
   double* d_table64 = nullptr;
+  double* d_tablek = nullptr;   // key-indexed copy [168][168][32] + 32 zeros
   double* d_lj_eps = nullptr;
   double* d_lj_sigma = nullptr;
   StepCtl* d_ctl = nullptr;
@@ -236,7 +237,7 @@ int setup_complex(sd_ctx* c, const sd_complex_desc& d, ComplexHost& h, int gbase
   D.ntiles = nslots / SD_TILE;
   h.nslots = nslots;
   std::vector<double> rxyz((size_t)nslots * 3, 0.0), rmodes((size_t)std::max(1, D.nmr) * nslots * 3, 0.0);
-  std::vector<int> rmask(nslots, 0), rrow(nslots, 0), rlj(nslots, 0);
+  std::vector<int> rmask(nslots, 0), rrow(nslots, 0), rrowk(nslots, 0), rlj(nslots, 0);
   std::vector<float> rq(nslots, 0.f);
   std::vector<float4> tiles(D.ntiles);
   for (int s = 0; s < nslots; ++s) {
@@ -248,6 +249,7 @@ int setup_complex(sd_ctx* c, const sd_complex_desc& d, ComplexHost& h, int gbase
         rmodes[((size_t)m * nslots + s) * 3 + k] = d.rec_modes[((size_t)m * d.n_rec + i) * 3 + k];
     rmask[s] = d.rec_mask[i];
     rrow[s] = d.rec_dfire_type[i] * SD_ROW;
+    rrowk[s] = d.rec_dfire_type[i] * SD_ROWK;
     if (d.rec_charge) rq[s] = (float)d.rec_charge[i];
     if (d.rec_lj_type) rlj[s] = d.rec_lj_type[i];
   }
@@ -312,6 +314,7 @@ int setup_complex(sd_ctx* c, const sd_complex_desc& d, ComplexHost& h, int gbase
   if ((rc = upload(c, h, rmodes.data(), rmodes.size(), &D.r_modes))) return rc;
   if ((rc = upload(c, h, rmask.data(), rmask.size(), &D.r_mask))) return rc;
   if ((rc = upload(c, h, rrow.data(), rrow.size(), &D.r_row))) return rc;
+  if ((rc = upload(c, h, rrowk.data(), rrowk.size(), &D.r_rowk))) return rc;
   if ((rc = upload(c, h, tiles.data(), tiles.size(), &D.r_tile))) return rc;
   if ((rc = upload(c, h, rq.data(), rq.size(), &D.r_q))) return rc;
   if ((rc = upload(c, h, rlj.data(), rlj.size(), &D.r_lj))) return rc;
@@ -348,7 +351,7 @@ int setup_complex(sd_ctx* c, const sd_complex_desc& d, ComplexHost& h, int gbase
     }
     const size_t nls = lslots.size();
     std::vector<double> cxyz(nls * 3, 0.0), cmodes((size_t)std::max(1, D.nml) * nls * 3, 0.0);
-    std::vector<int> cmask(nls, 0), ccol(nls, 0);
+    std::vector<int> cmask(nls, 0), ccol(nls, 0), ccolk(nls, 0);
     for (size_t s = 0; s < nls; ++s) {
       const int j = lslots[s];
       if (j < 0) continue;
@@ -357,6 +360,7 @@ int setup_complex(sd_ctx* c, const sd_complex_desc& d, ComplexHost& h, int gbase
         for (int k = 0; k < 3; ++k) cmodes[((size_t)m * nls + s) * 3 + k] = d.lig_modes[((size_t)m * d.n_lig + j) * 3 + k];
       cmask[s] = d.lig_mask[j];
       ccol[s] = d.lig_dfire_type[j] * SD_DFIRE_BINS;
+      ccolk[s] = d.lig_dfire_type[j] * SD_KEYS;
     }
     double lc[3] = {0, 0, 0};
     for (int j = 0; j < d.n_lig; ++j)
@@ -369,6 +373,7 @@ int setup_complex(sd_ctx* c, const sd_complex_desc& d, ComplexHost& h, int gbase
     if ((rc2 = upload(c, h, cmodes.data(), cmodes.size(), &D.lc_modes))) return rc2;
     if ((rc2 = upload(c, h, cmask.data(), cmask.size(), &D.lc_mask))) return rc2;
     if ((rc2 = upload(c, h, ccol.data(), ccol.size(), &D.lc_col))) return rc2;
+    if ((rc2 = upload(c, h, ccolk.data(), ccolk.size(), &D.lc_colk))) return rc2;
   }
   std::vector<int> lcol(d.n_lig), llj(d.n_lig, 0);
   std::vector<float> lq(d.n_lig, 0.f);
@@ -438,7 +443,7 @@ int rebuild_worklist(sd_ctx* c) {
 }
 
 int configure_score_v(sd_ctx* c, int precision, int variant, int* grid, size_t* smem) {
-  const size_t sm = score_smem_bytes(precision, c->scoring, c->max_nr, c->max_nl);
+  const size_t sm = score_smem_bytes(precision, c->scoring, c->max_nr, c->max_nl, variant);
   const void* k = score_kernel_ptr(precision, c->scoring, variant);
   const int threads = score_threads_of(precision, c->scoring, variant);
   SD_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(sm, 1)));
@@ -522,6 +527,7 @@ int autotune_mixed(sd_ctx* c) {
   L.ctl = c->d_ctl_scratch;
   L.work[0] = L.work[1] = (const int*)c->s_work.p;
   L.table64 = c->d_table64;
+  L.tablek = c->d_tablek;
   L.lj_eps = c->d_lj_eps;
   L.lj_sigma = c->d_lj_sigma;
   cudaEvent_t e0, e1;
@@ -570,6 +576,7 @@ int enqueue_step(sd_ctx* c, int precision, int grid, size_t sm) {
   L.work[0] = c->d_work[0];
   L.work[1] = c->d_work[1];
   L.table64 = c->d_table64;
+  L.tablek = c->d_tablek;
   L.lj_eps = c->d_lj_eps;
   L.lj_sigma = c->d_lj_sigma;
   L.energy_out = nullptr;
@@ -614,6 +621,7 @@ int ctx_noalloc_view(sd_ctx* c, int ci, int precision, DevComplex* desc, ScoreLa
   *desc = c->cx[ci].d;
   memset(L, 0, sizeof *L);
   L->table64 = c->d_table64;
+  L->tablek = c->d_tablek;
   L->lj_eps = c->d_lj_eps;
   L->lj_sigma = c->d_lj_sigma;
   *device = c->device;
@@ -658,7 +666,7 @@ int sd_ctx_create(const sd_complex_desc* complexes, int n_complexes, const sd_ta
   // device memory the context will hold (tables, per-complex data, state, work lists), checked
   // against SPARKLE_DEVICE_BUDGET_MB when set (a forced budget, e.g. to test the OOM path)
   {
-    size_t bytes = (size_t)(SD_TABLE_SIZE + 32) * 12 + 4096;
+    size_t bytes = (size_t)(SD_TABLE_SIZE + 32) * 12 + (size_t)(SD_TABLE_KEYS + 32) * 8 + 4096;
     for (int i = 0; i < n_complexes; ++i) {
       const sd_complex_desc& d = complexes[i];
       const size_t nr = (size_t)((d.n_rec + SD_TILE - 1) / SD_TILE) * SD_TILE, nl = (size_t)d.n_lig;
@@ -721,6 +729,7 @@ int sd_ctx_create(const sd_complex_desc* complexes, int n_complexes, const sd_ta
   if ((rc = cu(cudaMalloc(&c->d_cplx, sizeof(DevComplex) * n_complexes), "cudaMalloc"))) return bail(rc);
   if ((rc = cu(cudaMalloc(&c->d_cplx_scratch, sizeof(DevComplex) * n_complexes), "cudaMalloc"))) return bail(rc);
   if ((rc = cu(cudaMalloc(&c->d_table64, sizeof(double) * (SD_TABLE_SIZE + 32)), "cudaMalloc"))) return bail(rc);
+  if ((rc = cu(cudaMalloc(&c->d_tablek, sizeof(double) * (SD_TABLE_KEYS + 32)), "cudaMalloc"))) return bail(rc);
   if ((rc = cu(cudaMalloc(&c->d_lj_eps, sizeof(double) * SD_LJ_TYPES), "cudaMalloc"))) return bail(rc);
   if ((rc = cu(cudaMalloc(&c->d_lj_sigma, sizeof(double) * SD_LJ_TYPES), "cudaMalloc"))) return bail(rc);
   if ((rc = cu(cudaMalloc(&c->d_ctl, sizeof(StepCtl)), "cudaMalloc"))) return bail(rc);
@@ -734,6 +743,15 @@ int sd_ctx_create(const sd_complex_desc* complexes, int n_complexes, const sd_ta
       if (!std::isfinite(tables->dfire_energy[i])) return bail(fail(SD_ERR_NUMERIC, "non-finite DFIRE table entry"));
       t64[i] = tables->dfire_energy[i];
     }
+    // key-indexed copy: entry [tR][tL][k] is what the reference reads for key k, the flat index
+    // tR*3360 + tL*20 + dist_to_bins[k]-1 (key 29, d^2 == 225, reads bin 20: the next ligand
+    // type's bin 0, or the zero padding after the last type pair)
+    static const int kBin[30] = {0, 0, 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 13, 14, 14, 15, 15, 16, 16, 17, 17, 18, 18, 19, 19, 20};
+    std::vector<double> tk((size_t)SD_TABLE_KEYS + 32, 0.0);
+    for (int a = 0; a < SD_DFIRE_TYPES; ++a)
+      for (int b = 0; b < SD_DFIRE_TYPES; ++b)
+        for (int k = 0; k < 30; ++k)
+          tk[(size_t)a * SD_ROWK + b * SD_KEYS + k] = t64[(size_t)a * SD_ROW + b * SD_DFIRE_BINS + kBin[k]];
     std::vector<double> eps(SD_LJ_TYPES, 0.0), sig(SD_LJ_TYPES, 0.0);
     if (tables->lj_eps && tables->lj_sigma)
       for (int i = 0; i < SD_LJ_TYPES; ++i) {
@@ -746,6 +764,7 @@ int sd_ctx_create(const sd_complex_desc* complexes, int n_complexes, const sd_ta
     StepCtl ctl;
     memset(&ctl, 0, sizeof ctl);
     if ((rc = cu(cudaMemcpy(c->d_table64, t64.data(), t64.size() * 8, cudaMemcpyHostToDevice), "upload"))) return bail(rc);
+    if ((rc = cu(cudaMemcpy(c->d_tablek, tk.data(), tk.size() * 8, cudaMemcpyHostToDevice), "upload"))) return bail(rc);
     if ((rc = cu(cudaMemcpy(c->d_lj_eps, eps.data(), eps.size() * 8, cudaMemcpyHostToDevice), "upload"))) return bail(rc);
     if ((rc = cu(cudaMemcpy(c->d_lj_sigma, sig.data(), sig.size() * 8, cudaMemcpyHostToDevice), "upload"))) return bail(rc);
     if ((rc = cu(cudaMemcpy(c->d_swarm_map, smap.data(), smap.size() * 4, cudaMemcpyHostToDevice), "upload"))) return bail(rc);
@@ -764,7 +783,7 @@ int sd_ctx_destroy(sd_ctx* c) {
   if (c->graph) cudaGraphExecDestroy(c->graph);
   for (auto& h : c->cx)
     for (void* p : h.owned) cudaFree(p);
-  void* ps[] = {c->d_cplx, c->d_cplx_scratch, c->d_table64, c->d_lj_eps, c->d_lj_sigma, c->d_ctl,
+  void* ps[] = {c->d_cplx, c->d_cplx_scratch, c->d_table64, c->d_tablek, c->d_lj_eps, c->d_lj_sigma, c->d_ctl,
                 c->d_ctl_scratch, c->d_work[0], c->d_work[1], c->d_swarm_map, c->s_pose.p, c->s_score.p,
                 c->s_ref.p, c->s_energy.p, c->s_work.p, c->s_grad.p, c->s_bins.p};
   for (void* p : ps)
@@ -1014,6 +1033,7 @@ int sd_score_poses(sd_ctx* c, int ci, const double* poses, int n, int precision,
   L.work[0] = (const int*)c->s_work.p;
   L.work[1] = (const int*)c->s_work.p;
   L.table64 = c->d_table64;
+  L.tablek = c->d_tablek;
   L.lj_eps = c->d_lj_eps;
   L.lj_sigma = c->d_lj_sigma;
   L.energy_out = (double*)c->s_energy.p;
@@ -1094,6 +1114,7 @@ int sd_pydock_grad(sd_ctx* c, int ci, const double* poses, int n, int precision,
   L.work[0] = (const int*)c->s_work.p;
   L.work[1] = (const int*)c->s_work.p;
   L.table64 = c->d_table64;
+  L.tablek = c->d_tablek;
   L.lj_eps = c->d_lj_eps;
   L.lj_sigma = c->d_lj_sigma;
   L.energy_out = (double*)c->s_energy.p;

@@ -12,6 +12,9 @@
 
 #define SD_TABLE_SIZE (SD_DFIRE_TYPES * SD_DFIRE_TYPES * SD_DFIRE_BINS)
 #define SD_ROW (SD_DFIRE_TYPES * SD_DFIRE_BINS)  /* 3360 */
+#define SD_KEYS 32              /* bin keys per type pair in the key-indexed table (30 used) */
+#define SD_ROWK (SD_DFIRE_TYPES * SD_KEYS)        /* 5376 */
+#define SD_TABLE_KEYS (SD_DFIRE_TYPES * SD_ROWK)  /* key-indexed table entries, followed by 32 zeros */
 #define SD_CUTOFF2 225.0
 #define SD_MAX_COMPLEX 32
 #define SD_TILE 32              /* receptor atoms per tile (one warp lane each) */
@@ -45,6 +48,7 @@ struct DevComplex {
   const double* r_modes;   // [nmr][nslots][3]
   const int* r_mask;       // [nslots]
   const int* r_row;        // [nslots] DFIRE row base tR*3360
+  const int* r_rowk;       // [nslots] key-indexed row base tR*5376
   const float4* r_tile;    // [ntiles] centre (rest frame) + radius
   const float* r_q;        // [nslots] charge (pyDock)
   const int* r_lj;         // [nslots] LJ type (pyDock)
@@ -64,6 +68,7 @@ struct DevComplex {
   const double* lc_modes;  // [nml][nlchunks*32][3]
   const int* lc_mask;      // [nlchunks*32]
   const int* lc_col;       // [nlchunks*32]
+  const int* lc_colk;      // [nlchunks*32] key-indexed column base tL*32
   float lig_ctr[3];        // ligand centroid (ligand frame)
   float mnorm_r[SD_MAX_MODES], mnorm_l[SD_MAX_MODES];  // max per-atom mode norm (rounded up)
   float lig_radius;        // max |l0_j| (rounded up)
@@ -111,6 +116,7 @@ struct ScoreLaunch {
   StepCtl* ctl;
   const int* work[2];
   const double* table64;   // [SD_TABLE_SIZE + 32] zero padded
+  const double* tablek;    // [SD_TABLE_KEYS + 32] key-indexed: [tR][tL][key] = table64[tR*3360 + tL*20 + bin(key)]
   const double* lj_eps;    // [20] pyDock
   const double* lj_sigma;
   double* energy_out;      // nullable [local glowworm] raw energies (stateless scoring)
@@ -129,7 +135,7 @@ struct GsoLaunch {
 // kernel launchers (sd_score.cu, sd_gso.cu)
 int score_launch(const ScoreLaunch& L, int precision, int scoring, int grid, int threads, size_t smem,
                  cudaStream_t st, int variant);
-size_t score_smem_bytes(int precision, int scoring, int max_nr, int max_nl);
+size_t score_smem_bytes(int precision, int scoring, int max_nr, int max_nl, int variant);
 int score_threads_of(int precision, int scoring, int variant);
 const void* score_kernel_ptr(int precision, int scoring, int variant);
 int mixed_variant_count();

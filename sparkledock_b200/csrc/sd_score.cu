@@ -278,29 +278,30 @@ struct MixedVariant {
   const void* fn;
   int warps;
   int min_blocks;
+  size_t dyn_extra;  // dynamic shared memory in front of the ligand buffers
 };
+#define SD_RING(W, B, H, D, S, K) { (const void*)dfire_score_ring_kernel<W, B, H, D, S, K>, W, B, 0 }
 static const MixedVariant kMixedVariants[] = {
-    {(const void*)dfire_score_mixed_kernel<4, 4, true>, 4, 4},
-    {(const void*)dfire_score_ring_kernel<8, 3, true, true, false>, 8, 3},
-    {(const void*)dfire_score_ring_kernel<4, 5, true, true, false>, 4, 5},
-    {(const void*)dfire_score_ring_kernel<8, 3, true, true, true>, 8, 3},
-    {(const void*)dfire_score_ring_kernel<4, 5, true, true, true>, 4, 5},
-    {(const void*)dfire_score_ring_kernel<4, 4, true, true, true>, 4, 4},
-    {(const void*)dfire_score_ring_kernel<8, 3, true, false, true>, 8, 3},
-    {(const void*)dfire_score_ring_kernel<8, 2, true, true, true>, 8, 2},
-    {(const void*)dfire_score_ring_kernel<4, 5, false, true, true>, 4, 5},
+    {(const void*)dfire_score_mixed_kernel<4, 4, true>, 4, 4, 0},
+    SD_RING(8, 3, true, true, true, false),
+    SD_RING(8, 3, true, true, true, true),
+    SD_RING(8, 3, true, true, false, true),
+    SD_RING(4, 5, true, true, true, true),
+    SD_RING(4, 4, true, true, true, true),
+    SD_RING(8, 3, true, false, true, true),
+    SD_RING(4, 5, false, true, true, true),
 };
 constexpr int kNumMixedVariants = sizeof(kMixedVariants) / sizeof(kMixedVariants[0]);
 static_assert(kNumMixedVariants <= SD_MAX_VARIANTS, "variant table");
 
 static const MixedVariant& mixed_variant(int v) { return kMixedVariants[v < 0 || v >= kNumMixedVariants ? 0 : v]; }
 
-size_t score_smem_bytes(int precision, int scoring, int max_nr, int max_nl) {
+size_t score_smem_bytes(int precision, int scoring, int max_nr, int max_nl, int variant) {
   if (scoring == SD_SCORING_PYDOCK) return pydock_smem_bytes(precision, false, max_nl, max_nr);
   if (precision == SD_PREC_MIXED) {
     const size_t nlc = (size_t)(max_nl + SD_TILE - 1) / SD_TILE;
     const size_t ntiles = (size_t)(max_nr + SD_TILE - 1) / SD_TILE;
-    return (size_t)16 * (nlc * SD_TILE + nlc) + 4 * (3 * ntiles + nlc);
+    return mixed_variant(variant).dyn_extra + (size_t)16 * (nlc * SD_TILE + nlc) + 4 * (3 * ntiles + nlc);
   }
   return (size_t)16 * ((max_nl + 1) & ~1) + (size_t)32 * max_nl + (size_t)8 * max_nr +
          (size_t)4 * ((max_nr + SD_TILE - 1) / SD_TILE);

@@ -32,6 +32,7 @@ namespace {
 
 constexpr int kRingCap = 1088;  // < 64 left over + at most 32 x 32 from one batch
 constexpr int kZeroIdx = SD_TABLE_SIZE + 8;  // a zero in the table padding
+constexpr int kZeroIdxKey = SD_TABLE_KEYS;   // a zero past the key-indexed table
 
 // exact_pair_key (sd_score_mixed.cuh) inlined: measured fewer spills here than the call
 __device__ __forceinline__ int exact_pair_key_inline(const DevComplex* C, int nslots, const double* pose,
@@ -67,7 +68,10 @@ struct __align__(16) RingBufs {
 // kDual: stage 2 takes 64 ring entries per round, two per lane (else 32, one per lane).
 // kSoA: candidate buffers as separate x / y / z / col arrays (conflict-free 4-byte reads in stage
 // 2) instead of one float4 per candidate.
-template <int kWarps, int kMinBlocks, bool kH16, bool kDual, bool kSoA>
+// kKey: gather from the key-indexed table [168][168][32] (the bin mapping folded in, including
+// the reference's d^2 == 225 read of the next ligand type's bin 0) and test the bin edges
+// ((k+1)/2)^2 arithmetically, instead of three per-key shared-memory tables.
+template <int kWarps, int kMinBlocks, bool kH16, bool kDual, bool kSoA, bool kKey>
 __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_ring_kernel(ScoreLaunch L) {
   constexpr int kG = kDual ? 64 : 32;  // entries per stage-2 round
   constexpr int kSortMax = 512;        // near tiles ordered largest-first up to this many
@@ -110,43 +114,63 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_ring_kern
     const double* pose_g = C.pos + (size_t)p * pl;
     if (tid < pl) sh_pose[tid] = pose_g[tid];
     __syncthreads();
-    if (tid == 0) {
-      for (int k = 0; k < 4; ++k) sh_q[k] = sh_pose[3 + k];
-      quat_inverse(sh_q, sh_qi);
-      float dR = 0.f, dL = 0.f;
-      for (int m = 0; m < C.nmr; ++m) dR += fabsf((float)sh_pose[7 + m]) * C.mnorm_r[m];
-      for (int m = 0; m < C.nml; ++m) dL += fabsf((float)sh_pose[7 + C.nmr + m]) * C.mnorm_l[m];
-      dR = dR * 1.0001f + 1e-4f;
-      dL = dL * 1.0001f + 1e-4f;
-      sh_bound[0] = dR;
-      sh_bound[1] = dL;
-      // bound of |FP32 d2 - FP64 d2| for pairs within 15.1 A (coordinates centred on t)
-      const float RL = C.lig_radius + dL;
-      const float u32 = 5.9604645e-8f;
-      sh_bound[2] = 2.0f * (2.02f * u32 * (26.2f * (2.0f * RL + 15.1f) + 228.0f) + 3.0f * u32 * 228.0f) + 1e-6f;
-      const double n = sqrt(sh_q[0] * sh_q[0] + sh_q[1] * sh_q[1] + sh_q[2] * sh_q[2] + sh_q[3] * sh_q[3]);
-      const float w0 = (float)(sh_q[0] / n), x = (float)(sh_q[1] / n), y = (float)(sh_q[2] / n),
-                  z = (float)(sh_q[3] / n);
-      sh_rot[0] = 1 - 2 * (y * y + z * z);
-      sh_rot[1] = 2 * (x * y - w0 * z);
-      sh_rot[2] = 2 * (x * z + w0 * y);
-      sh_rot[3] = 2 * (x * y + w0 * z);
-      sh_rot[4] = 1 - 2 * (x * x + z * z);
-      sh_rot[5] = 2 * (y * z - w0 * x);
-      sh_rot[6] = 2 * (x * z - w0 * y);
-      sh_rot[7] = 2 * (y * z + w0 * x);
-      sh_rot[8] = 1 - 2 * (x * x + y * y);
-      for (int a = 0; a < 3; ++a)
-        sh_gc[a] = sh_rot[3 * a] * C.lig_ctr[0] + sh_rot[3 * a + 1] * C.lig_ctr[1] + sh_rot[3 * a + 2] * C.lig_ctr[2];
-      // ligand reference point (prepare_gso_tasks.cc:460, :513, :524-526)
-      double rx = C.lig_ref[0], ry = C.lig_ref[1], rz = C.lig_ref[2];
-      quat_rotate(sh_q, sh_qi, rx, ry, rz);
-      double* ref = C.ref + (size_t)p * 3;
-      ref[0] = rx + sh_pose[0];
-      ref[1] = ry + sh_pose[1];
-      ref[2] = rz + sh_pose[2];
-      sh_ntile = 0;
-      sh_next = 0;
+    if (warp == 0) {
+      // pose prologue spread over warp 0: quaternion inverse (one division per lane, bit-identical
+      // to quat_inverse), FP32 rotation for culling, ANM displacement bounds, reference point
+      if (lane < 4) {
+        const double w0 = sh_pose[3], x = sh_pose[4], y = sh_pose[5], z = sh_pose[6];
+        const double n2 = w0 * w0 + x * x + y * y + z * z;
+        const double qv = sh_pose[3 + lane];
+        sh_q[lane] = qv;
+        sh_qi[lane] = (lane == 0 ? qv : -qv) / n2;
+      }
+      {
+        const float qw = (float)sh_pose[3], qx = (float)sh_pose[4], qy = (float)sh_pose[5], qz = (float)sh_pose[6];
+        const float in = rsqrtf(qw * qw + qx * qx + qy * qy + qz * qz);
+        const float w0 = qw * in, x = qx * in, y = qy * in, z = qz * in;
+        float rv = 0.f;
+        switch (lane) {
+          case 0: rv = 1 - 2 * (y * y + z * z); break;
+          case 1: rv = 2 * (x * y - w0 * z); break;
+          case 2: rv = 2 * (x * z + w0 * y); break;
+          case 3: rv = 2 * (x * y + w0 * z); break;
+          case 4: rv = 1 - 2 * (x * x + z * z); break;
+          case 5: rv = 2 * (y * z - w0 * x); break;
+          case 6: rv = 2 * (x * z - w0 * y); break;
+          case 7: rv = 2 * (y * z + w0 * x); break;
+          case 8: rv = 1 - 2 * (x * x + y * y); break;
+          default: break;
+        }
+        if (lane < 9) sh_rot[lane] = rv;
+      }
+      float tR = lane < C.nmr ? fabsf((float)sh_pose[7 + lane]) * C.mnorm_r[lane] : 0.f;
+      float tL = lane < C.nml ? fabsf((float)sh_pose[7 + C.nmr + lane]) * C.mnorm_l[lane] : 0.f;
+      for (int o = 16; o > 0; o >>= 1) {
+        tR += __shfl_xor_sync(0xffffffffu, tR, o);
+        tL += __shfl_xor_sync(0xffffffffu, tL, o);
+      }
+      __syncwarp();
+      if (lane < 3)
+        sh_gc[lane] = sh_rot[3 * lane] * C.lig_ctr[0] + sh_rot[3 * lane + 1] * C.lig_ctr[1] +
+                      sh_rot[3 * lane + 2] * C.lig_ctr[2];
+      if (lane == 0) {
+        const float dR = tR * 1.0001f + 1e-4f, dL = tL * 1.0001f + 1e-4f;
+        sh_bound[0] = dR;
+        sh_bound[1] = dL;
+        // bound of |FP32 d2 - FP64 d2| for pairs within 15.1 A (coordinates centred on t)
+        const float RL = C.lig_radius + dL;
+        const float u32 = 5.9604645e-8f;
+        sh_bound[2] = 2.0f * (2.02f * u32 * (26.2f * (2.0f * RL + 15.1f) + 228.0f) + 3.0f * u32 * 228.0f) + 1e-6f;
+        // ligand reference point (prepare_gso_tasks.cc:460, :513, :524-526)
+        double rx = C.lig_ref[0], ry = C.lig_ref[1], rz = C.lig_ref[2];
+        quat_rotate(sh_q, sh_qi, rx, ry, rz);
+        double* ref = C.ref + (size_t)p * 3;
+        ref[0] = rx + sh_pose[0];
+        ref[1] = ry + sh_pose[1];
+        ref[2] = rz + sh_pose[2];
+        sh_ntile = 0;
+        sh_next = 0;
+      }
     }
     __syncthreads();
     const double tx = sh_pose[0], ty = sh_pose[1], tz = sh_pose[2];
@@ -179,31 +203,30 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_ring_kern
       const float cx = (float)((double)tile.x - tx), cy = (float)((double)tile.y - ty),
                   cz = (float)((double)tile.z - tz);
       const float reach = 15.0f + dR + SD_CULL_MARGIN + tile.w + lig_reach;
-      if (cx * cx + cy * cy + cz * cz <= reach * reach) tlist[atomicAdd(&sh_ntile, 1)] = k;
+      if (cx * cx + cy * cy + cz * cz <= reach * reach) {
+        // distance from the ligand centroid: the closest tiles have the most pairs
+        const int at = atomicAdd(&sh_ntile, 1);
+        const float ex = cx - sh_gc[0], ey = cy - sh_gc[1], ez = cz - sh_gc[2];
+        tlist[at] = k;
+        tdist[at] = ex * ex + ey * ey + ez * ez;
+      }
     }
     __syncthreads();
     const int ntile = sh_ntile;
     const bool sorted = ntile <= kSortMax;
-    // distance of each near tile from the ligand centroid (closest tiles have the most pairs),
-    // and which ligand chunks any near tile can reach (the same test as the per-tile one below,
-    // with 0.01 A to spare, so a chunk that is not needed is never read)
-    for (int t = tid; t < ntile; t += blockDim.x) {
-      const float4 tile = C.r_tile[tlist[t]];
-      const float ex = (float)((double)tile.x - tx) - sh_gc[0], ey = (float)((double)tile.y - ty) - sh_gc[1],
-                  ez = (float)((double)tile.z - tz) - sh_gc[2];
-      tdist[t] = ex * ex + ey * ey + ez * ez;
-    }
-    for (int i = tid; i < ntile * nlc; i += blockDim.x) {
-      const int t = i / nlc, c = i - t * nlc;
+    // which ligand chunks any near tile can reach (the same test as the per-tile one below, with
+    // 0.01 A to spare, so a chunk that is not needed is never read)
+    for (int t = warp; t < ntile; t += kWarps) {
       const float4 tile = C.r_tile[tlist[t]];
       const float cx = (float)((double)tile.x - tx), cy = (float)((double)tile.y - ty),
                   cz = (float)((double)tile.z - tz);
-      const float4 ch = chS[c];
-      const float ex = ch.x - cx, ey = ch.y - cy, ez = ch.z - cz,
-                  r = (15.0f + dR + SD_CULL_MARGIN + tile.w) + ch.w + 0.01f;
-      if (ex * ex + ey * ey + ez * ez <= r * r) cneed[c] = 1;
+      const float rt = 15.0f + dR + SD_CULL_MARGIN + tile.w;
+      for (int c = lane; c < nlc; c += 32) {
+        const float4 ch = chS[c];
+        const float ex = ch.x - cx, ey = ch.y - cy, ez = ch.z - cz, r = rt + ch.w + 0.01f;
+        if (ex * ex + ey * ey + ez * ez <= r * r) cneed[c] = 1;
+      }
     }
-    __syncthreads();
     if (sorted) {
       for (int t = tid; t < ntile; t += blockDim.x) {
         const float d = tdist[t];
@@ -215,21 +238,28 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_ring_kern
         tord[rank] = tlist[t];
       }
     }
-    for (int s = tid; s < nls; s += blockDim.x) {
-      if (!cneed[s >> 5]) continue;
+    __syncthreads();
+    auto lig_atom = [&](int s) {
+      if (s >= nls || !cneed[s >> 5]) return;
       if (C.l_perm[s] >= 0) {
         double x, y, z;
         ligand_exact_chunk(C, s, sh_pose, sh_q, sh_qi, x, y, z);
-        ligS[s] = make_float4((float)(x - tx), (float)(y - ty), (float)(z - tz), __int_as_float(C.lc_col[s]));
+        ligS[s] = make_float4((float)(x - tx), (float)(y - ty), (float)(z - tz),
+                              __int_as_float(kKey ? C.lc_colk[s] : C.lc_col[s]));
       } else {
         ligS[s] = make_float4(1e18f, 1e18f, 1e18f, __int_as_float(0));
       }
+    };
+    for (int s = tid; s < nls; s += 2 * kWarps * 32) {
+      lig_atom(s);
+      lig_atom(s + kWarps * 32);
     }
     __syncthreads();
     const int* tl = sorted ? tord : tlist;
     const float cut2 = 225.0f + B;
     double acc = 0.0;               // per-lane FP64 sum of table values
-    double pv0 = 0.0, pv1 = 0.0;    // values gathered by the previous drain, added by the next
+    double pv0 = 0.0, pv1 = 0.0;    // values gathered by the previous round, added by the next
+    const double* table = kKey ? L.tablek : L.table64;
     unsigned npairs = 0, nevals = 0;
 
     for (;;) {
@@ -253,7 +283,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_ring_kern
         fx = (float)(rx - tx);
         fy = (float)(ry - ty);
         fz = (float)(rz - tz);
-        row = C.r_row[slot];
+        row = kKey ? C.r_rowk[slot] : C.r_row[slot];
       }
       W.rec[lane] = make_float4(fx, fy, fz, __int_as_float(row));
       const unsigned act_mask = __ballot_sync(0xffffffffu, active);
@@ -404,7 +434,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_ring_kern
         // stage 2: drain whole rounds of kG; everything at the end of the tile, or when entries
         // of the previous batch would otherwise outlive its buffer
         const int upto = (final_batch || (oldL > 0 && head < kG)) ? head : (head & ~(kG - 1));
-        auto pair = [&](int t0, int h, int n) -> double {
+        auto pair = [&](int t0, int h, int n) -> int {
           const unsigned e = W.ring[t0 + h * 32 + lane];
           const int cix = (int)(e >> 5) & 63, rl = (int)e & 31;
           float4 lf;
@@ -421,8 +451,20 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_ring_kern
           // key estimate; d2 == 0 gives NaN -> 0 and lies within B of edge 0 (exact path)
           const float r = d2 * rsqrtf(d2);
           const int key = (int)fmaf(r, 2.0f, -1.0f) & 31;
-          int idx = __float_as_int(rr.w) + __float_as_int(lf.w) + sh_kbin[key];
-          if (ok && (d2 <= sh_klo[key] || d2 >= sh_khi[key])) {
+          int idx;
+          bool near;
+          if (kKey) {
+            // key edges ((key+1)/2)^2 and ((key+2)/2)^2, differences with one rounding; the upper
+            // edge stops at the cutoff 15^2, so key 29 (d^2 == 225 only) always takes the exact
+            // path: the FP32 cut2 = 225 + B may round above 225 + B
+            idx = __float_as_int(rr.w) + __float_as_int(lf.w) + key;
+            const float h = fmaf((float)key, 0.5f, 0.5f), h1 = fminf(h + 0.5f, 15.0f);
+            near = fmaf(-h, h, d2) <= B || fmaf(h1, h1, -d2) <= B;
+          } else {
+            idx = __float_as_int(rr.w) + __float_as_int(lf.w) + sh_kbin[key];
+            near = d2 <= sh_klo[key] || d2 >= sh_khi[key];
+          }
+          if (ok && near) {
             atomicAdd(&sh_cnt[0], 1ull);
             int edge;
             const int kx = exact_pair_key_inline(&C, nslots, sh_pose, sh_q, sh_qi, sh_T, k * SD_TILE + rl,
@@ -430,20 +472,20 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_ring_kern
             if (kx < 0) {
               ok = false;
             } else {
-              idx = __float_as_int(rr.w) + __float_as_int(lf.w) + c_binlut[kx];
+              idx = __float_as_int(rr.w) + __float_as_int(lf.w) + (kKey ? kx : c_binlut[kx]);
               if (edge) atomicAdd(&sh_cnt[edge], 1ull);
             }
           }
           npairs += ok ? 1u : 0u;
-          return __ldg(L.table64 + (ok ? idx : kZeroIdx));
+          return ok ? idx : (kKey ? kZeroIdxKey : kZeroIdx);
         };
         for (int t0 = 0; t0 < upto; t0 += kG) {
-          acc += pv0;
           const int n = min(kG, upto - t0);
-          pv0 = pair(t0, 0, n);
+          acc += pv0;
+          pv0 = __ldg(table + pair(t0, 0, n));
           if (kDual) {
             acc += pv1;
-            pv1 = pair(t0, 1, n);
+            pv1 = __ldg(table + pair(t0, 1, n));
           }
         }
         // move the leftover (< kG) entries to the front

@@ -174,3 +174,81 @@ def test_every_mixed_kernel_variant(variant, c0, tables, monkeypatch):
         st = dk.stats()
         assert st["guard_errors"] == 0
         assert st["pairs_in_cutoff"] > 0
+
+
+def _edge_sweep_complex():
+    """One receptor atom at the origin and one ligand atom at the ligand-frame origin; every other
+    atom more than 100 A away, so each pose has exactly one candidate pair, at distance |t|."""
+    cx = sd.SyntheticComplex(40, 30, 1, 4, n_modes_rec=0, n_modes_lig=0, seed=3)
+    for i in range(cx.n_rec):
+        cx.rec_xyz[i] = (-100.0 - 3.0 * i, 0.0, 0.0)
+    for j in range(cx.n_lig):
+        cx.lig_xyz[j] = (100.0 + 3.0 * j, 0.0, 0.0)
+    cx.rec_xyz[0] = (0.0, 0.0, 0.0)
+    cx.lig_xyz[0] = (0.0, 0.0, 0.0)
+    d = [np.sqrt(((k + 1) / 2.0) ** 2) * (1.0 + m * 1e-7) for k in range(1, 30) for m in range(-60, 61, 4)]
+    d += [15.0 + m * 1e-6 for m in range(-150, 151, 3)]
+    d += [0.05 * m for m in range(1, 12)]
+    poses = np.zeros((len(d), cx.pose_len))
+    poses[:, 0] = d
+    poses[:, 3] = 1.0
+    return cx, np.concatenate([poses, _cutoff_window_poses(cx)])
+
+
+def _cutoff_window_poses(cx):
+    """Poses whose FP32 pair distance lands exactly on the mixed kernel's FP32 cutoff
+    cut2 = 225 + B and on its neighbouring floats (B, the FP32 error bound, evaluated in the
+    kernel's operation order).  d2 = fma(ey, ey, ex * ex) for the pair (rec atom 0 at the origin,
+    ligand atom 0 at t, coordinates centred on t)."""
+    f = np.float32
+    lr = float(np.sqrt((cx.lig_xyz ** 2).sum(1)).max()) * (1 + 1e-6) + 1e-4
+    lig_radius = f(lr)
+    if float(lig_radius) < lr:
+        lig_radius = np.nextafter(lig_radius, f(np.inf))
+    u = f(5.9604645e-8)
+    RL = f(lig_radius + f(1e-4))                 # dL = 0 * 1.0001 + 1e-4 without modes
+    t4 = f(f(f(26.2) * f(f(f(2.0) * RL) + f(15.1))) + f(228.0))
+    B = f(f(f(2.0) * f(f(f(f(2.02) * u) * t4) + f(f(f(3.0) * u) * f(228.0)))) + f(1e-6))
+    cut2 = f(f(225.0) + B)
+    targets = {float(cut2)}
+    x = cut2
+    for _ in range(3):
+        x = np.nextafter(x, f(np.inf)); targets.add(float(x))
+    x = cut2
+    for _ in range(3):
+        x = np.nextafter(x, f(0)); targets.add(float(x))
+    out = []
+    tx0 = f(np.sqrt(np.float64(cut2)))
+    for k in range(-40, 41):
+        ex = f(tx0 + f(k) * f(9.5367432e-07))
+        p = f(np.float64(ex) * np.float64(ex))
+        for ey in (0.0, 1e-3, 2e-3, 3e-3, 4e-3, 6e-3, 8e-3, 1.1e-2):
+            ey = f(ey)
+            d2 = f(np.float64(ey) * np.float64(ey) + np.float64(p))
+            if float(d2) in targets:
+                pose = np.zeros(cx.pose_len)
+                pose[0], pose[1], pose[3] = -float(ex), -float(ey), 1.0
+                out.append(pose)
+                targets.discard(float(d2))
+    assert float(cut2) not in targets, "no pose lands on the FP32 cutoff"
+    return np.array(out)
+
+
+@pytest.mark.parametrize("variant", range(sd.mixed_variant_count()))
+def test_single_pair_sweep_across_bin_edges(variant, tables, monkeypatch):
+    """A single pair swept across every DFIRE bin edge and across the cutoff within the FP32 error
+    bound: each compiled mixed variant gives the oracle's energy for every distance (a wrong bin or
+    a pair counted past the cutoff shows up as an O(1) error), and FP64 is bit-identical."""
+    monkeypatch.setenv("SPARKLE_MIXED_VARIANT", str(variant))
+    cx, poses = _edge_sweep_complex()
+    _, ref_en = oracle_scores(OracleSystem(cx, tables), poses)
+    with sd.Docking([cx], tables, precision=sd.SD_PREC_MIXED) as dk:
+        dk.init_state(0, np.tile(poses[:1], (cx.n_swarms * cx.n_glowworms, 1)).reshape(cx.poses.shape))
+        dk.set_draws(0, sd.gso_draws(0, cx.n_swarms, 1, cx.n_glowworms))
+        dk.step(1)  # selects the forced variant
+        assert dk.tuning()["variant"] == variant
+        _, en = dk.score_poses(0, poses, sd.SD_PREC_MIXED)
+        assert np.abs(en - ref_en).max() <= 1e-12, np.nonzero(np.abs(en - ref_en) > 1e-12)
+        _, en64 = dk.score_poses(0, poses, sd.SD_PREC_FP64)
+        assert np.array_equal(en64, ref_en)
+        assert dk.stats()["pairs_fallback"] > 0
