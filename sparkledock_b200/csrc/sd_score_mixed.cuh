@@ -1,68 +1,56 @@
-// Mixed-precision DFIRE scoring (FP16/FP32 distances, exact bins, FP64 sums of table values).
-// Included by sd_score.cu (shares its constant-memory key thresholds and bin table).
+// Mixed-precision DFIRE scoring (included by sd_score.cu: shares its constant-memory key
+// thresholds and exact_key).
 //
-// Same contract as the FP64 kernels in sd_score.cu (energy of cdfire_calculate_dfire,
-// prepare_gso_tasks.cc:1522-1615, with every bin identical to the FP64 reference bin), but the
-// summation order is free, which this kernel uses:
-//  * the ligand is kept in spatial chunks of 32 atoms (k-d order, ligand frame); a receptor
-//    tile (one warp, one lane per receptor atom) rejects whole ligand chunks by bounding
-//    spheres, then single atoms by ballot, and collects the surviving ligand atoms as
-//    candidates;
-//  * stage 1 takes candidates 32 at a time: their coordinates are staged once in a per-warp
-//    buffer, every lane tests its receptor atom against all 32 (fully unrolled, broadcast
-//    reads) and keeps a 32-bit in-cutoff mask; one warp scan per batch then appends the
-//    in-cutoff pairs (ligand slot, lane) to a per-warp ring;
-//  * stage 2 drains the ring 64 pairs at a time, two per lane: recompute d^2 (same FP32
-//    expression, so the same value), key from a fast reciprocal square root, the exact-bin
-//    guard against the proven FP32 error bound B, two table gathers in flight, and each lane
-//    adds the FP64 table value of its pairs with one FP64 add.  The FP64 pipe is otherwise
-//    idle here; compensated FP32 (Kahan) sums were measured to leave ~2e-5 absolute error at
-//    60k pairs per pose, because every compensation step rounds the incoming value, and they
-//    cost five FP32 adds per pair.
-//    Pairs within B of a bin edge or of the cutoff are recomputed from the exact FP64 pose
-//    transform (counted as fallbacks).
+// Same contract as the FP64 kernels: the energy of cdfire_calculate_dfire
+// (prepare_gso_tasks.cc:1522-1615) with every bin identical to the FP64 reference bin, FP64 sums
+// of FP64 table values, but in a free order, which the kernel uses:
+//  * persistent CTAs grab poses from the device work list; per pose the ligand is transformed
+//    (exact FP64, rounded to FP32 centred on the pose translation t) only for the spatial chunks
+//    of 32 atoms that some receptor tile within reach can reach, and the near receptor tiles are
+//    ordered largest-first (closest to the ligand centroid) so warps finish a pose together;
+//  * a warp takes a receptor tile (one lane per atom, FP64 ANM transform rounded to FP32),
+//    rejects ligand chunks by bounding spheres and ligand atoms by ballot, and stages the
+//    surviving candidates 32 at a time into one of two per-warp batch buffers, in the bit order
+//    of the stage-1 mask (candidate 2i at position i, 2i+1 at position 16+i);
+//  * stage 1 (kH16) tests a pair with the dot-product form of the distance in packed FP16,
+//    three HFMA2 per two candidates: s = r.l - |l|^2/2 >= (|r|^2 - thr)/2, on coordinates
+//    centred on the tile centre.  thr is set per tile from a proven bound on the FP16 error
+//    (below), so every pair whose FP32 d^2 is within the cutoff passes; tiles or poses whose
+//    magnitudes would make the bound loose pass every candidate, and stage 2 filters exactly.
+//    Without kH16 the test is the FP32 d^2 itself;
+//  * in-cutoff pairs are appended to a per-warp ring of 16-bit entries (buffer, position,
+//    receptor lane) by a warp scan; stage 2 drains it 32 or 64 entries per round (kDual: two per
+//    lane), reads the candidate and the receptor atom from 4-byte arrays and a float4 (mostly
+//    broadcast reads), recomputes the FP32 d^2 and takes the key from a fast reciprocal square
+//    root.  The key's edges ((k+1)/2)^2 and ((k+2)/2)^2 (the upper one stopped at the cutoff) are
+//    compared with d^2 - edge computed with one rounding against the FP32 error bound B, so a
+//    pair that is not near an edge has its FP64 bin proven; near pairs are recomputed from the
+//    exact FP64 transform (counted as fallbacks);
+//  * the table is gathered from a key-indexed copy [168][168][32] (entry k is the value the
+//    reference reads for key k, including the d^2 == 225 read of the next ligand type's bin 0),
+//    so no bin lookup is needed; a rejected or padding pair gathers a zero past the table instead
+//    of branching, and each round's gathers are added by the next round, so they are in flight
+//    while the next round is evaluated.  Each lane sums its values in FP64 (Kahan sums of an
+//    FP32-rounded table were measured to miss 1e-5 at 60k pairs per pose); warp shuffles and a
+//    block reduction in FP64 finish the pose.
+//
+// FP16 bound (u = 2^-11, R >= |r - c| for the tile's atoms, Lb >= |l - c| for its candidates,
+// w = |l - c|^2 / 2):  |s_fp16 - (r.l - w)| <= u (2.001 R Lb + w) + 3u (1.002 R Lb + 1.001 w)
+// <= u (5.1 R Lb + 2.1 Lb^2) = Es, and the right-hand side rounds by at most u (R^2 + thr)/2 = Ea,
+// so thr = 225 + B + 2 Es + 2 Ea + 0.01 keeps every pair with FP32 d^2 <= 225 + B.
 #pragma once
 
 namespace sd {
 namespace {
 
-constexpr int kRing = 1024;  // per-warp ring of in-cutoff pairs (a batch adds at most 32*32)
+constexpr int kRingCap = 1088;  // < 64 left over + at most 32 x 32 from one batch
+constexpr int kZeroIdxKey = SD_TABLE_KEYS;   // a zero past the key-indexed table
 
-struct __align__(16) WarpBufs {
-  float4 cand_xyz[32];   // staged candidate ligand atoms (centred FP32, col bits)
-  __half cand_h[16][8];  // FP16 pre-filter: per candidate pair {x0,x1,y0,y1,z0,z1,-,-}, tile-centred
-  int cand_slot[64];     // pending candidate ligand slots
-  float rx[32], ry[32], rz[32];  // this tile's receptor atoms (centred FP32); SoA: one bank per lane
-  int rrow[32];
-  int ring[kRing];       // packed (ligand slot << 5 | lane)
-};
-
-__device__ __forceinline__ int exact_key_m(double d2, const double* T) {
-  float f = sqrtf((float)d2) * 2.0f - 1.0f;
-  int k = (int)f;
-  k = k < 0 ? 0 : (k > 29 ? 29 : k);
-  if (k < 29 && d2 >= T[k + 1]) ++k;
-  else if (k > 0 && d2 < T[k]) --k;
-  return k;
-}
-
-struct PoseCtx {
-  const DevComplex* C;
-  int nslots;
-  const double* pose;
-  const double* q;
-  const double* qi;
-  const double* T;
-  const float4* key4;  // per key: {lower threshold, upper threshold, bin bits, 0}
-  const double* table;  // FP64 DFIRE table: one 8-byte gather per pair
-  float B;
-};
-
-// exact FP64 key of one pair near a bin edge or the cutoff (rare: kept out of line so that its
-// registers do not weigh on the hot loop); returns -1 when the pair is outside the cutoff and
-// sets *edge to 1 for d^2 == 0, 2 for d^2 == 225
-__device__ __noinline__ int exact_pair_key(const DevComplex* C, int nslots, const double* pose, const double* q,
-                                           const double* qi, const double* T, int slot, int j, int* edge) {
+// exact FP64 key of one pair near a bin edge or the cutoff; -1 when the pair is outside the
+// cutoff; *edge = 1 for d^2 == 0, 2 for d^2 == 225 (inlined: measured fewer spills than a call)
+__device__ __forceinline__ int exact_pair_key(const DevComplex* C, int nslots, const double* pose,
+                                                     const double* q, const double* qi, const double* T, int slot,
+                                                     int j, int* edge) {
   double rx, ry, rz, lx, ly, lz;
   receptor_exact(*C, nslots, slot, pose, rx, ry, rz);
   ligand_exact(*C, j, pose, q, qi, lx, ly, lz);
@@ -74,71 +62,50 @@ __device__ __noinline__ int exact_pair_key(const DevComplex* C, int nslots, cons
     *edge = 1;
     return 0;
   }
-  const int key = exact_key_m(e2, T);
+  const int key = exact_key(e2, T);
   if (key == 29) *edge = 2;
   return key;
 }
 
-// value of one in-cutoff candidate pair (slot = receptor slot, ls = ligand chunk slot);
-// returns false when the exact FP64 distance shows the pair is outside the cutoff
-__device__ __forceinline__ bool pair_value(const PoseCtx& P, float d2, int base, int slot, int ls, double& val,
-                                           unsigned long long& nfb, unsigned long long& nz, unsigned long long& ncut) {
-  // key estimate; d2 == 0 gives NaN -> 0 and is caught by the edge guard below
-  const float r = d2 * rsqrtf(d2);
-  int key = (int)fmaf(r, 2.0f, -1.0f);
-  key = key < 0 ? 0 : (key > 29 ? 29 : key);
-  const float4 kk = P.key4[key];
-  int bin = __float_as_int(kk.z);
-  const bool near = (d2 - kk.x <= P.B) || (kk.y - d2 <= P.B);
-  if (near) {
-    ++nfb;
-    int edge;
-    key = exact_pair_key(P.C, P.nslots, P.pose, P.q, P.qi, P.T, slot, P.C->l_perm[ls], &edge);
-    if (key < 0) return false;
-    nz += edge == 1;
-    ncut += edge == 2;
-    bin = __float_as_int(P.key4[key].z);
-  }
-  val = P.table[base + bin];
-  return true;
-}
+struct __align__(16) RingBufs {
+  float candf[4][64];        // x, y, z, col bits of [buffer][position]: ligand atom centred on t
+  __half candh[16][8];       // position pair i: {x(2i), x(2i+1), y.., y.., z.., z.., -w.., -w..}
+  float4 rec[32];            // receptor atom of each lane centred on t, row bits
+  int cslot[64];             // [buffer][position]: ligand chunk slot (exact fallback only)
+  int pend[64];              // pending candidate ligand slots
+  unsigned short ring[kRingCap];  // (buffer << 10) | (position << 5) | lane
+};
 
 }  // namespace
 
-// kH16: stage 1 tests candidate pairs two at a time in packed FP16 on tile-centred coordinates
-// against 229 A^2, a superset of the FP32 test (FP16 error on d^2 <= 1.75 A^2 for pairs within
-// the cutoff: |coordinates| <= 22.5 A after centring, 2^-11 rounding per conversion and
-// subtraction, half an ulp of 256 per multiply-add); stage 2 recomputes d^2 in FP32 and keeps
-// only d^2 <= 225 + B, so the result is identical to the FP32 pre-filter.
-template <int kWarps, int kMinBlocks, bool kH16>
+// kH16: packed-FP16 stage-1 test (else FP32).  kDual: stage 2 takes 64 ring entries per round,
+// two per lane (else 32, one per lane).
+template <int kWarps, int kMinBlocks, bool kH16, bool kDual>
 __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_kernel(ScoreLaunch L) {
+  constexpr int kG = kDual ? 64 : 32;  // entries per stage-2 round
+  constexpr int kSortMax = 512;        // near tiles ordered largest-first up to this many
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ WarpBufs wb[kWarps];
+  __shared__ RingBufs wb[kWarps];
   __shared__ double sh_pose[7 + 2 * SD_MAX_MODES];
   __shared__ double sh_q[4], sh_qi[4];
   __shared__ double sh_T[32];
-  __shared__ float4 sh_key4[32];
-  __shared__ double sh_red[32];
-  __shared__ int sh_item;
-  __shared__ int sh_ntile, sh_next;
+  __shared__ float sh_gc[3];      // ligand centroid, rotated (centred on t)
+  __shared__ double sh_red[kWarps];
+  __shared__ int sh_item, sh_ntile, sh_next;
   __shared__ float sh_bound[4];
   __shared__ float sh_rot[9];
-  __shared__ unsigned long long sh_fallback, sh_z, sh_cut, sh_pairs, sh_evals;
+  __shared__ unsigned long long sh_cnt[5];  // fallback, d2 == 0, d2 == 225, pairs, evaluations
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  if (tid < 32) {
-    sh_T[tid] = c_T[tid];
-    const int k = tid < 30 ? tid : 29;
-    sh_key4[tid] = make_float4(c_Tf[k], c_Tf[k + 1], __int_as_float(c_binlut[k]), 0.f);
-  }
-  if (tid == 0) sh_fallback = sh_z = sh_cut = sh_pairs = sh_evals = 0;
+  if (tid < 32) sh_T[tid] = c_T[tid];
+  if (tid < 5) sh_cnt[tid] = 0;
   StepCtl* ctl = L.ctl;
   const int parity = ctl->parity;
   const int count = ctl->count[parity];
   const int* work = L.work[parity];
-  unsigned long long n_done = 0, nfb = 0, nz = 0, ncut = 0, npairs = 0, nevals = 0, nguard = 0;
+  unsigned n_done = 0;
   const unsigned lt_mask = (1u << lane) - 1u;
-  WarpBufs& W = wb[warp];
+  RingBufs& W = wb[warp];
 
   for (;;) {
     __syncthreads();
@@ -149,90 +116,156 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
     const int w = work[item];
     const int ci = wi_complex(w), p = wi_local(w);
     const DevComplex& C = L.cplx[ci];
-    const int nslots = nslots_of(C), pl = C.pl, nlc = C.nlchunks, nls = nlc * SD_TILE;
+    const int nslots = nslots_of(C), pl = C.pl, nlc = C.nlchunks;
     const double* pose_g = C.pos + (size_t)p * pl;
     if (tid < pl) sh_pose[tid] = pose_g[tid];
     __syncthreads();
-    if (tid == 0) {
-      for (int k = 0; k < 4; ++k) sh_q[k] = sh_pose[3 + k];
-      quat_inverse(sh_q, sh_qi);
-      float dR = 0.f, dL = 0.f;
-      for (int m = 0; m < C.nmr; ++m) dR += fabsf((float)sh_pose[7 + m]) * C.mnorm_r[m];
-      for (int m = 0; m < C.nml; ++m) dL += fabsf((float)sh_pose[7 + C.nmr + m]) * C.mnorm_l[m];
-      dR = dR * 1.0001f + 1e-4f;
-      dL = dL * 1.0001f + 1e-4f;
-      sh_bound[0] = dR;
-      sh_bound[1] = dL;
-      // bound of |FP32 d2 - FP64 d2| for pairs within 15.1 A (coordinates centred on t)
-      const float RL = C.lig_radius + dL;
-      const float u32 = 5.9604645e-8f;
-      sh_bound[2] = 2.0f * (2.02f * u32 * (26.2f * (2.0f * RL + 15.1f) + 228.0f) + 3.0f * u32 * 228.0f) + 1e-6f;
-      // rotation matrix of the unit quaternion (chunk centres only; the culling margin covers it)
-      const double n = sqrt(sh_q[0] * sh_q[0] + sh_q[1] * sh_q[1] + sh_q[2] * sh_q[2] + sh_q[3] * sh_q[3]);
-      const float w0 = (float)(sh_q[0] / n), x = (float)(sh_q[1] / n), y = (float)(sh_q[2] / n),
-                  z = (float)(sh_q[3] / n);
-      sh_rot[0] = 1 - 2 * (y * y + z * z);
-      sh_rot[1] = 2 * (x * y - w0 * z);
-      sh_rot[2] = 2 * (x * z + w0 * y);
-      sh_rot[3] = 2 * (x * y + w0 * z);
-      sh_rot[4] = 1 - 2 * (x * x + z * z);
-      sh_rot[5] = 2 * (y * z - w0 * x);
-      sh_rot[6] = 2 * (x * z - w0 * y);
-      sh_rot[7] = 2 * (y * z + w0 * x);
-      sh_rot[8] = 1 - 2 * (x * x + y * y);
-      // ligand reference point (prepare_gso_tasks.cc:460, :513, :524-526)
-      double rx = C.lig_ref[0], ry = C.lig_ref[1], rz = C.lig_ref[2];
-      quat_rotate(sh_q, sh_qi, rx, ry, rz);
-      double* ref = C.ref + (size_t)p * 3;
-      ref[0] = rx + sh_pose[0];
-      ref[1] = ry + sh_pose[1];
-      ref[2] = rz + sh_pose[2];
-      sh_ntile = 0;
-      sh_next = 0;
+    if (warp == 0) {
+      // pose prologue spread over warp 0: quaternion inverse (one division per lane, bit-identical
+      // to quat_inverse), FP32 rotation for culling, ANM displacement bounds, reference point
+      if (lane < 4) {
+        const double w0 = sh_pose[3], x = sh_pose[4], y = sh_pose[5], z = sh_pose[6];
+        const double n2 = w0 * w0 + x * x + y * y + z * z;
+        const double qv = sh_pose[3 + lane];
+        sh_q[lane] = qv;
+        sh_qi[lane] = (lane == 0 ? qv : -qv) / n2;
+      }
+      {
+        const float qw = (float)sh_pose[3], qx = (float)sh_pose[4], qy = (float)sh_pose[5], qz = (float)sh_pose[6];
+        const float in = rsqrtf(qw * qw + qx * qx + qy * qy + qz * qz);
+        const float w0 = qw * in, x = qx * in, y = qy * in, z = qz * in;
+        float rv = 0.f;
+        switch (lane) {
+          case 0: rv = 1 - 2 * (y * y + z * z); break;
+          case 1: rv = 2 * (x * y - w0 * z); break;
+          case 2: rv = 2 * (x * z + w0 * y); break;
+          case 3: rv = 2 * (x * y + w0 * z); break;
+          case 4: rv = 1 - 2 * (x * x + z * z); break;
+          case 5: rv = 2 * (y * z - w0 * x); break;
+          case 6: rv = 2 * (x * z - w0 * y); break;
+          case 7: rv = 2 * (y * z + w0 * x); break;
+          case 8: rv = 1 - 2 * (x * x + y * y); break;
+          default: break;
+        }
+        if (lane < 9) sh_rot[lane] = rv;
+      }
+      float tR = lane < C.nmr ? fabsf((float)sh_pose[7 + lane]) * C.mnorm_r[lane] : 0.f;
+      float tL = lane < C.nml ? fabsf((float)sh_pose[7 + C.nmr + lane]) * C.mnorm_l[lane] : 0.f;
+      for (int o = 16; o > 0; o >>= 1) {
+        tR += __shfl_xor_sync(0xffffffffu, tR, o);
+        tL += __shfl_xor_sync(0xffffffffu, tL, o);
+      }
+      __syncwarp();
+      if (lane < 3)
+        sh_gc[lane] = sh_rot[3 * lane] * C.lig_ctr[0] + sh_rot[3 * lane + 1] * C.lig_ctr[1] +
+                      sh_rot[3 * lane + 2] * C.lig_ctr[2];
+      if (lane == 0) {
+        const float dR = tR * 1.0001f + 1e-4f, dL = tL * 1.0001f + 1e-4f;
+        sh_bound[0] = dR;
+        sh_bound[1] = dL;
+        // bound of |FP32 d2 - FP64 d2| for pairs within 15.1 A (coordinates centred on t)
+        const float RL = C.lig_radius + dL;
+        const float u32 = 5.9604645e-8f;
+        sh_bound[2] = 2.0f * (2.02f * u32 * (26.2f * (2.0f * RL + 15.1f) + 228.0f) + 3.0f * u32 * 228.0f) + 1e-6f;
+        // ligand reference point (prepare_gso_tasks.cc:460, :513, :524-526)
+        double rx = C.lig_ref[0], ry = C.lig_ref[1], rz = C.lig_ref[2];
+        quat_rotate(sh_q, sh_qi, rx, ry, rz);
+        double* ref = C.ref + (size_t)p * 3;
+        ref[0] = rx + sh_pose[0];
+        ref[1] = ry + sh_pose[1];
+        ref[2] = rz + sh_pose[2];
+        sh_ntile = 0;
+        sh_next = 0;
+      }
     }
     __syncthreads();
     const double tx = sh_pose[0], ty = sh_pose[1], tz = sh_pose[2];
-    const float dR = sh_bound[0], dL = sh_bound[1];
-    float4* ligS = reinterpret_cast<float4*>(smem);  // [nlc*32] centred, col bits
-    float4* chS = ligS + (size_t)nlc * SD_TILE;      // [nlc] centre + radius
+    const float dR = sh_bound[0], dL = sh_bound[1], B = sh_bound[2];
+    const int nls = nlc * SD_TILE, ntiles = C.ntiles;
+    float4* ligS = reinterpret_cast<float4*>(smem);  // [nls] centred on t, col bits
+    float4* chS = ligS + nls;                        // [nlc] centre + radius
     int* tlist = reinterpret_cast<int*>(chS + nlc);  // [ntiles] tiles within reach
-    for (int s = tid; s < nlc * SD_TILE; s += blockDim.x) {
-      const int j = C.l_perm[s];
-      if (j >= 0) {
-        double x, y, z;
-        ligand_exact(C, j, sh_pose, sh_q, sh_qi, x, y, z);
-        ligS[s] = make_float4((float)(x - tx), (float)(y - ty), (float)(z - tz), __int_as_float(C.l_col[j]));
-      } else {
-        ligS[s] = make_float4(1e18f, 1e18f, 1e18f, __int_as_float(0));
-      }
-    }
+    int* tord = tlist + ntiles;                      // [ntiles] the same, largest first
+    float* tdist = reinterpret_cast<float*>(tord + ntiles);  // [ntiles]
+    int* cneed = reinterpret_cast<int*>(tdist + ntiles);     // [nlc] chunk within reach of a near tile
     for (int c = tid; c < nlc; c += blockDim.x) {
       const float4 cc = C.l_chunk[c];
       const float X = sh_rot[0] * cc.x + sh_rot[1] * cc.y + sh_rot[2] * cc.z;
       const float Y = sh_rot[3] * cc.x + sh_rot[4] * cc.y + sh_rot[5] * cc.z;
       const float Z = sh_rot[6] * cc.x + sh_rot[7] * cc.y + sh_rot[8] * cc.z;
       chS[c] = make_float4(X, Y, Z, cc.w + dL);
+      cneed[c] = 0;
     }
     const float lig_reach = C.lig_radius + dL;
-    for (int k = tid; k < C.ntiles; k += blockDim.x) {
+    for (int k = tid; k < ntiles; k += blockDim.x) {
       const float4 tile = C.r_tile[k];
       const float cx = (float)((double)tile.x - tx), cy = (float)((double)tile.y - ty),
                   cz = (float)((double)tile.z - tz);
       const float reach = 15.0f + dR + SD_CULL_MARGIN + tile.w + lig_reach;
-      if (cx * cx + cy * cy + cz * cz <= reach * reach) tlist[atomicAdd(&sh_ntile, 1)] = k;
+      if (cx * cx + cy * cy + cz * cz <= reach * reach) {
+        // distance from the ligand centroid: the closest tiles have the most pairs
+        const int at = atomicAdd(&sh_ntile, 1);
+        const float ex = cx - sh_gc[0], ey = cy - sh_gc[1], ez = cz - sh_gc[2];
+        tlist[at] = k;
+        tdist[at] = ex * ex + ey * ey + ez * ez;
+      }
     }
     __syncthreads();
     const int ntile = sh_ntile;
-    PoseCtx P{&C, nslots, sh_pose, sh_q, sh_qi, sh_T, sh_key4, L.table64, sh_bound[2]};
-    const float cut2 = 225.0f + P.B;
-    double acc = 0.0;  // per-thread FP64 sum of the table values of its pairs
+    const bool sorted = ntile <= kSortMax;
+    // which ligand chunks any near tile can reach (the same test as the per-tile one below, with
+    // 0.01 A to spare, so a chunk that is not needed is never read)
+    for (int t = warp; t < ntile; t += kWarps) {
+      const float4 tile = C.r_tile[tlist[t]];
+      const float cx = (float)((double)tile.x - tx), cy = (float)((double)tile.y - ty),
+                  cz = (float)((double)tile.z - tz);
+      const float rt = 15.0f + dR + SD_CULL_MARGIN + tile.w;
+      for (int c = lane; c < nlc; c += 32) {
+        const float4 ch = chS[c];
+        const float ex = ch.x - cx, ey = ch.y - cy, ez = ch.z - cz, r = rt + ch.w + 0.01f;
+        if (ex * ex + ey * ey + ez * ez <= r * r) cneed[c] = 1;
+      }
+    }
+    if (sorted) {
+      for (int t = tid; t < ntile; t += blockDim.x) {
+        const float d = tdist[t];
+        int rank = 0;
+        for (int u = 0; u < ntile; ++u) {
+          const float e = tdist[u];
+          rank += (e < d || (e == d && u < t)) ? 1 : 0;
+        }
+        tord[rank] = tlist[t];
+      }
+    }
+    __syncthreads();
+    auto lig_atom = [&](int s) {
+      if (s >= nls || !cneed[s >> 5]) return;
+      if (C.l_perm[s] >= 0) {
+        double x, y, z;
+        ligand_exact_chunk(C, s, sh_pose, sh_q, sh_qi, x, y, z);
+        ligS[s] = make_float4((float)(x - tx), (float)(y - ty), (float)(z - tz), __int_as_float(C.lc_colk[s]));
+      } else {
+        ligS[s] = make_float4(1e18f, 1e18f, 1e18f, __int_as_float(0));
+      }
+    };
+    for (int s = tid; s < nls; s += 2 * kWarps * 32) {
+      lig_atom(s);
+      lig_atom(s + kWarps * 32);
+    }
+    __syncthreads();
+    const int* tl = sorted ? tord : tlist;
+    const float cut2 = 225.0f + B;
+    double acc = 0.0;               // per-lane FP64 sum of table values
+    double pv0 = 0.0, pv1 = 0.0;    // values gathered by the previous round, added by the next
+    const double* table = L.tablek;
+    unsigned npairs = 0, nevals = 0;
 
     for (;;) {
       int ti = 0;
       if (lane == 0) ti = atomicAdd(&sh_next, 1);
       ti = __shfl_sync(0xffffffffu, ti, 0);
       if (ti >= ntile) break;
-      const int k = tlist[ti];
+      const int k = tl[ti];
       const float4 tile = C.r_tile[k];
       const float cx = (float)((double)tile.x - tx), cy = (float)((double)tile.y - ty),
                   cz = (float)((double)tile.z - tz);
@@ -248,176 +281,210 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
         fx = (float)(rx - tx);
         fy = (float)(ry - ty);
         fz = (float)(rz - tz);
-        row = C.r_row[slot];
+        row = C.r_rowk[slot];
       }
-      W.rx[lane] = fx;
-      W.ry[lane] = fy;
-      W.rz[lane] = fz;
-      W.rrow[lane] = row;
-      const int nact = __popc(__ballot_sync(0xffffffffu, active));
-      int ncand = 0, head = 0, tail = 0;  // warp-uniform
+      W.rec[lane] = make_float4(fx, fy, fz, __int_as_float(row));
+      const unsigned act_mask = __ballot_sync(0xffffffffu, active);
+      const int nact = __popc(act_mask);
+      // stage-1 constants of this lane
+      __half2 rx2, ry2, rz2, a2;
+      const float R = tile.w + dR + SD_CULL_MARGIN, Lb = reach + 0.01f;
+      const bool tight = R <= 40.0f && Lb <= 80.0f;  // warp-uniform
+      if (kH16) {
+        const float u16 = 4.8828125e-4f;
+        const float Es = u16 * (5.1f * R * Lb + 2.1f * Lb * Lb);
+        const float thr0 = 225.0f + B + 1e-3f + 2.0f * Es;
+        const float thr = thr0 + u16 * (R * R + thr0 + 10.0f) + 2e-4f + 0.01f;
+        const float ux = fx - cx, uy = fy - cy, uz = fz - cz;
+        const float a = 0.5f * (ux * ux + uy * uy + uz * uz) - 0.5f * thr;
+        const bool use = active && tight;
+        rx2 = __float2half2_rn(use ? ux : 0.f);
+        ry2 = __float2half2_rn(use ? uy : 0.f);
+        rz2 = __float2half2_rn(use ? uz : 0.f);
+        // loose tile: every candidate passes (s = 0 > -65504); inactive lane: none does
+        a2 = __float2half2_rn(!active ? 65504.f : (tight ? a : -65504.f));
+      }
+      int ncand = 0, head = 0, par = 0, oldL = 0;  // ring holds entries [0, head)
+      int cb = 0;
+      unsigned cm = 0;
 
-      // stage 2: consume n (<= 64) ring entries, two per lane
-      auto drain = [&](int n) {
-        const int i0 = tail + lane, i1 = tail + 32 + lane;
-        const bool v0 = lane < n, v1 = lane + 32 < n;
-        double a0 = 0.0, a1 = 0.0;
-        bool k0 = false, k1 = false;
-        if (v0) {
-          const int e = W.ring[i0 & (kRing - 1)];
-          const int ls = e >> 5, rl = e & 31;
-          if ((unsigned)ls >= (unsigned)nls) {  // guard: never taken unless the ring is corrupt
-            ++nguard;
-          } else {
-          const float4 Lg = ligS[ls];
-          const float ex = W.rx[rl] - Lg.x, ey = W.ry[rl] - Lg.y, ez = W.rz[rl] - Lg.z;
-          const float d2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
-          if (d2 <= cut2)
-            k0 = pair_value(P, d2, W.rrow[rl] + __float_as_int(Lg.w), k * SD_TILE + rl, ls, a0, nfb, nz, ncut);
+      for (;;) {
+        // collect candidates until a batch is full or the ligand is exhausted
+        while (ncand < 32) {
+          if (cm == 0) {
+            if (cb >= nlc) break;
+            const int c = cb + lane;
+            bool cnear = false;
+            if (c < nlc) {
+              const float4 ch = chS[c];
+              const float ex = ch.x - cx, ey = ch.y - cy, ez = ch.z - cz, r = reach + ch.w;
+              cnear = ex * ex + ey * ey + ez * ez <= r * r;  // same expression as the cneed test
+            }
+            cm = __ballot_sync(0xffffffffu, cnear);
+            cb += 32;
+            continue;
           }
-        }
-        if (v1) {
-          const int e = W.ring[i1 & (kRing - 1)];
-          const int ls = e >> 5, rl = e & 31;
-          if ((unsigned)ls >= (unsigned)nls) {  // guard: never taken unless the ring is corrupt
-            ++nguard;
-          } else {
-          const float4 Lg = ligS[ls];
-          const float ex = W.rx[rl] - Lg.x, ey = W.ry[rl] - Lg.y, ez = W.rz[rl] - Lg.z;
-          const float d2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
-          if (d2 <= cut2)
-            k1 = pair_value(P, d2, W.rrow[rl] + __float_as_int(Lg.w), k * SD_TILE + rl, ls, a1, nfb, nz, ncut);
-          }
-        }
-        if (k0) {
-          acc += a0;
-          ++npairs;
-        }
-        if (k1) {
-          acc += a1;
-          ++npairs;
-        }
-        tail += n;
-      };
-      // stage 1: test the first 32 pending candidates against every lane's receptor atom
-      auto batch = [&](int nb) {
-        __syncwarp();
-        unsigned m = 0;
-        if (!kH16) {
-          // unused candidate places sit at -1e18, inactive receptor lanes at +1e18: never in range
-          if (lane < nb) W.cand_xyz[lane] = ligS[W.cand_slot[lane]];
-          else W.cand_xyz[lane] = make_float4(-1e18f, -1e18f, -1e18f, 0.f);
-          __syncwarp();
-#pragma unroll
-          for (int b = 0; b < 32; ++b) {
-            const float4 l = W.cand_xyz[b];
-            const float ex = fx - l.x, ey = fy - l.y, ez = fz - l.z;
-            const float d2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
-            m |= (d2 <= cut2 ? 1u : 0u) << b;
-          }
-          // only real candidates and real receptor atoms may produce pairs
-          m &= active ? (nb >= 32 ? 0xffffffffu : ((1u << nb) - 1u)) : 0u;
-        } else {
-          // candidate 2i in the low half, 2i+1 in the high half of pair slot i; unused places
-          // at -1000 and inactive receptor lanes at +inf (1e18 overflows): never in range
-          __half hx = __float2half_rn(-1000.f), hy = hx, hz = hx;
-          if (lane < nb) {
-            const float4 l = ligS[W.cand_slot[lane]];
-            hx = __float2half_rn(l.x - cx);
-            hy = __float2half_rn(l.y - cy);
-            hz = __float2half_rn(l.z - cz);
-          }
-          __half* q = W.cand_h[lane >> 1];
-          q[0 + (lane & 1)] = hx;
-          q[2 + (lane & 1)] = hy;
-          q[4 + (lane & 1)] = hz;
-          __syncwarp();
-          const __half2 rx2 = __half2half2(__float2half_rn(fx - cx));
-          const __half2 ry2 = __half2half2(__float2half_rn(fy - cy));
-          const __half2 rz2 = __half2half2(__float2half_rn(fz - cz));
-          const __half2 th2 = __float2half2_rn(229.0f);
-          unsigned M = 0;
-#pragma unroll
-          for (int i = 0; i < 16; ++i) {
-            const uint4 qq = *reinterpret_cast<const uint4*>(W.cand_h[i]);
-            const __half2 dx = __hsub2(rx2, *reinterpret_cast<const __half2*>(&qq.x));
-            const __half2 dy = __hsub2(ry2, *reinterpret_cast<const __half2*>(&qq.y));
-            const __half2 dz = __hsub2(rz2, *reinterpret_cast<const __half2*>(&qq.z));
-            const __half2 d2 = __hfma2(dz, dz, __hfma2(dy, dy, __hmul2(dx, dx)));
-            M |= __hle2_mask(d2, th2) & (0x00010001u << i);
-          }
-          // back to candidate order: bit i -> 2i, bit 16+i -> 2i+1
-          unsigned lo = M & 0xffffu, hi = M >> 16;
-          lo = (lo | (lo << 8)) & 0x00ff00ffu;
-          lo = (lo | (lo << 4)) & 0x0f0f0f0fu;
-          lo = (lo | (lo << 2)) & 0x33333333u;
-          lo = (lo | (lo << 1)) & 0x55555555u;
-          hi = (hi | (hi << 8)) & 0x00ff00ffu;
-          hi = (hi | (hi << 4)) & 0x0f0f0f0fu;
-          hi = (hi | (hi << 2)) & 0x33333333u;
-          hi = (hi | (hi << 1)) & 0x55555555u;
-          m = lo | (hi << 1);
-          m &= active ? (nb >= 32 ? 0xffffffffu : ((1u << nb) - 1u)) : 0u;
-        }
-        nevals += (unsigned long long)(lane == 0 ? nb * nact : 0);
-        // exclusive scan of the per-lane pair counts
-        const int cnt = __popc(m);
-        int incl = cnt;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int v = __shfl_up_sync(0xffffffffu, incl, o);
-          if (lane >= o) incl += v;
-        }
-        const int total = __shfl_sync(0xffffffffu, incl, 31);
-        if (head - tail + total > kRing)  // only for very dense batches: empty the ring first
-          while (head - tail > 0) drain(min(64, head - tail));
-        int pos = head + incl - cnt;
-        while (m) {
-          const int b = __ffs(m) - 1;
-          m &= m - 1;
-          W.ring[pos & (kRing - 1)] = (W.cand_slot[b] << 5) | lane;
-          ++pos;
-        }
-        head += total;
-        __syncwarp();
-        // keep the candidates beyond the first 32
-        const int rest = ncand - nb;
-        int carry = 0;
-        if (lane < rest) carry = W.cand_slot[32 + lane];
-        __syncwarp();
-        if (lane < rest) W.cand_slot[lane] = carry;
-        ncand = rest;
-        __syncwarp();
-        while (head - tail >= 64) drain(64);
-      };
-
-      for (int cb = 0; cb < nlc; cb += 32) {
-        const int c = cb + lane;
-        bool cnear = false;
-        if (c < nlc) {
-          const float4 ch = chS[c];
-          const float ex = ch.x - cx, ey = ch.y - cy, ez = ch.z - cz, r = reach + ch.w;
-          cnear = ex * ex + ey * ey + ez * ez <= r * r;
-        }
-        unsigned cm = __ballot_sync(0xffffffffu, cnear);
-        while (cm) {
-          const int cc = cb + __ffs(cm) - 1;
+          const int sb = (cb - 32 + __ffs(cm) - 1) * SD_TILE;
           cm &= cm - 1;
-          const int sb = cc * SD_TILE;
           const float4 la = ligS[sb + lane];
           const float ax = la.x - cx, ay = la.y - cy, az = la.z - cz;
-          const bool cand = ax * ax + ay * ay + az * az <= reach2;
+          const bool cand = fmaf(az, az, fmaf(ay, ay, ax * ax)) <= reach2;
           const unsigned am = __ballot_sync(0xffffffffu, cand);
-          if (cand) W.cand_slot[ncand + __popc(am & lt_mask)] = sb + lane;
+          if (cand) W.pend[ncand + __popc(am & lt_mask)] = sb + lane;
           ncand += __popc(am);
-          if (ncand >= 32) batch(32);
         }
+        const bool exhausted = cm == 0 && cb >= nlc;
+        if (ncand == 0 && head == 0) break;
+        const int nb = min(ncand, 32);
+        const bool final_batch = exhausted && ncand <= 32;
+        if (nb > 0) {
+          // stage the batch into buffer par, in mask bit order
+          __syncwarp();
+          const int pos = (lane >> 1) | ((lane & 1) << 4);
+          float4 l4 = make_float4(-1e18f, -1e18f, -1e18f, 0.f);
+          int s = 0;
+          if (lane < nb) {
+            s = W.pend[lane];
+            l4 = ligS[s];
+          }
+          W.candf[0][par * 32 + pos] = l4.x;
+          W.candf[1][par * 32 + pos] = l4.y;
+          W.candf[2][par * 32 + pos] = l4.z;
+          W.candf[3][par * 32 + pos] = l4.w;
+          W.cslot[par * 32 + pos] = s;
+          if (kH16) {
+            // unused place: s = -60000, never in range; loose tile: every place passes
+            float lx = 0.f, ly = 0.f, lz = 0.f, nw = tight ? -60000.f : 0.f;
+            if (lane < nb && tight) {
+              lx = l4.x - cx;
+              ly = l4.y - cy;
+              lz = l4.z - cz;
+              nw = fmaxf(-0.5f * (lx * lx + ly * ly + lz * lz), -60000.f);
+            }
+            __half* q = W.candh[lane >> 1];
+            q[0 + (lane & 1)] = __float2half_rn(lx);
+            q[2 + (lane & 1)] = __float2half_rn(ly);
+            q[4 + (lane & 1)] = __float2half_rn(lz);
+            q[6 + (lane & 1)] = __float2half_rn(nw);
+          }
+          __syncwarp();
+          // stage 1: bit b of m <=> (this lane's receptor atom, candidate at position b) in range
+          unsigned M = 0;
+          if (kH16) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+              const uint4 qq = *reinterpret_cast<const uint4*>(W.candh[i]);
+              __half2 sv = __hfma2(rx2, *reinterpret_cast<const __half2*>(&qq.x), *reinterpret_cast<const __half2*>(&qq.w));
+              sv = __hfma2(ry2, *reinterpret_cast<const __half2*>(&qq.y), sv);
+              sv = __hfma2(rz2, *reinterpret_cast<const __half2*>(&qq.z), sv);
+              M |= __hge2_mask(sv, a2) & (0x00010001u << i);
+            }
+          } else {
+#pragma unroll
+            for (int b = 0; b < 32; ++b) {
+              const float lx = W.candf[0][par * 32 + b], ly = W.candf[1][par * 32 + b],
+                          lz = W.candf[2][par * 32 + b];
+              const float ex = fx - lx, ey = fy - ly, ez = fz - lz;
+              const float d2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
+              M |= (d2 <= cut2 ? 1u : 0u) << b;
+            }
+          }
+          const unsigned lo = (1u << ((nb + 1) >> 1)) - 1u, hi = (1u << (nb >> 1)) - 1u;
+          unsigned m = M & (lo | (hi << 16)) & (active ? 0xffffffffu : 0u);
+          nevals += lane == 0 ? (unsigned)(nb * nact) : 0u;
+          // append this lane's pairs to the ring
+          const int cnt = __popc(m);
+          int incl = cnt;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+          }
+          const int total = __shfl_sync(0xffffffffu, incl, 31);
+          int at = head + incl - cnt;
+          const unsigned tag = ((unsigned)par << 10) | (unsigned)lane;
+          while (m) {
+            const int b = 31 - __clz(m);
+            m ^= 1u << b;
+            W.ring[at++] = (unsigned short)(tag | ((unsigned)b << 5));
+          }
+          head += total;
+          // keep the candidates beyond the first 32
+          const int rest = ncand - nb;
+          int carry = 0;
+          if (lane < rest) carry = W.pend[32 + lane];
+          __syncwarp();
+          if (lane < rest) W.pend[lane] = carry;
+          ncand = rest;
+          par ^= 1;
+        }
+        __syncwarp();
+        // stage 2: drain whole rounds of kG; everything at the end of the tile, or when entries
+        // of the previous batch would otherwise outlive its buffer
+        const int upto = (final_batch || (oldL > 0 && head < kG)) ? head : (head & ~(kG - 1));
+        auto pair = [&](int t0, int h, int n) -> int {
+          const unsigned e = W.ring[t0 + h * 32 + lane];
+          const int cix = (int)(e >> 5) & 63, rl = (int)e & 31;
+          const float4 rr = W.rec[rl];
+          const float ex = rr.x - W.candf[0][cix], ey = rr.y - W.candf[1][cix], ez = rr.z - W.candf[2][cix];
+          const int col = __float_as_int(W.candf[3][cix]);
+          const float d2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
+          bool ok = (h * 32 + lane < n) && d2 <= cut2;
+          // key estimate; d2 == 0 gives NaN -> 0 and lies within B of edge 0 (exact path)
+          const float r = d2 * rsqrtf(d2);
+          const int key = (int)fmaf(r, 2.0f, -1.0f) & 31;
+          // key edges ((key+1)/2)^2 and ((key+2)/2)^2, differences with one rounding; the upper
+          // edge stops at the cutoff 15^2, so key 29 (d^2 == 225 only) always takes the exact
+          // path: the FP32 cut2 = 225 + B may round above 225 + B
+          int idx = __float_as_int(rr.w) + col + key;
+          const float hk = fmaf((float)key, 0.5f, 0.5f), hk1 = fminf(hk + 0.5f, 15.0f);
+          const bool near = fmaf(-hk, hk, d2) <= B || fmaf(hk1, hk1, -d2) <= B;
+          if (ok && near) {
+            atomicAdd(&sh_cnt[0], 1ull);
+            int edge;
+            const int kx = exact_pair_key(&C, nslots, sh_pose, sh_q, sh_qi, sh_T, k * SD_TILE + rl,
+                                          C.l_perm[W.cslot[cix]], &edge);
+            if (kx < 0) {
+              ok = false;
+            } else {
+              idx = __float_as_int(rr.w) + col + kx;
+              if (edge) atomicAdd(&sh_cnt[edge], 1ull);
+            }
+          }
+          npairs += ok ? 1u : 0u;
+          return ok ? idx : kZeroIdxKey;
+        };
+        for (int t0 = 0; t0 < upto; t0 += kG) {
+          const int n = min(kG, upto - t0);
+          acc += pv0;
+          pv0 = __ldg(table + pair(t0, 0, n));
+          if (kDual) {
+            acc += pv1;
+            pv1 = __ldg(table + pair(t0, 1, n));
+          }
+        }
+        // move the leftover (< kG) entries to the front
+        const int left = head - upto;
+        unsigned short e0 = 0, e1 = 0;
+        if (lane < left) e0 = W.ring[upto + lane];
+        if (lane + 32 < left) e1 = W.ring[upto + 32 + lane];
+        __syncwarp();
+        if (lane < left) W.ring[lane] = e0;
+        if (lane + 32 < left) W.ring[lane + 32] = e1;
+        head = left;
+        oldL = left;
+        if (final_batch) break;
       }
-      if (ncand > 0) batch(ncand);
-      while (head - tail > 0) drain(min(64, head - tail));
       __syncwarp();
     }
-    // FP64 block reduction of the per-thread sums
+    acc += pv0;
+    acc += pv1;
+    // counters, then the FP64 block reduction of the per-lane sums
+    const unsigned wp = __reduce_add_sync(0xffffffffu, npairs);
+    if (lane == 0) {
+      if (wp) atomicAdd(&sh_cnt[3], (unsigned long long)wp);
+      if (nevals) atomicAdd(&sh_cnt[4], (unsigned long long)nevals);
+    }
     double v = acc;
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     if (lane == 0) sh_red[warp] = v;
@@ -431,20 +498,14 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
       ++n_done;
     }
   }
-  if (nfb) atomicAdd(&sh_fallback, nfb);
-  if (nz) atomicAdd(&sh_z, nz);
-  if (ncut) atomicAdd(&sh_cut, ncut);
-  if (npairs) atomicAdd(&sh_pairs, npairs);
-  if (nevals) atomicAdd(&sh_evals, nevals);
-  if (nguard) atomicAdd(&ctl->stats[ST_GUARD], nguard);
   __syncthreads();
   if (tid == 0) {
-    if (n_done) atomicAdd(&ctl->stats[ST_SCORED], n_done);
-    if (sh_fallback) atomicAdd(&ctl->stats[ST_FALLBACK], sh_fallback);
-    if (sh_z) atomicAdd(&ctl->stats[ST_D2ZERO], sh_z);
-    if (sh_cut) atomicAdd(&ctl->stats[ST_D2CUT], sh_cut);
-    if (sh_pairs) atomicAdd(&ctl->stats[ST_PAIRS], sh_pairs);
-    if (sh_evals) atomicAdd(&ctl->stats[ST_EVALS], sh_evals);
+    if (n_done) atomicAdd(&ctl->stats[ST_SCORED], (unsigned long long)n_done);
+    if (sh_cnt[0]) atomicAdd(&ctl->stats[ST_FALLBACK], sh_cnt[0]);
+    if (sh_cnt[1]) atomicAdd(&ctl->stats[ST_D2ZERO], sh_cnt[1]);
+    if (sh_cnt[2]) atomicAdd(&ctl->stats[ST_D2CUT], sh_cnt[2]);
+    if (sh_cnt[3]) atomicAdd(&ctl->stats[ST_PAIRS], sh_cnt[3]);
+    if (sh_cnt[4]) atomicAdd(&ctl->stats[ST_EVALS], sh_cnt[4]);
   }
 }
 
