@@ -252,3 +252,25 @@ def test_single_pair_sweep_across_bin_edges(variant, tables, monkeypatch):
         _, en64 = dk.score_poses(0, poses, sd.SD_PREC_FP64)
         assert np.array_equal(en64, ref_en)
         assert dk.stats()["pairs_fallback"] > 0
+
+
+@pytest.mark.parametrize("variant", range(sd.mixed_variant_count()))
+def test_large_anm_extents_loose_tiles(variant, tables, monkeypatch):
+    """Poses with ANM extents large enough that the displacement bound makes the FP16 stage-1
+    error bound too wide (tile bound R > 40 A): those tiles pass every candidate and stage 2
+    filters exactly; energies still match the FP64 oracle, and FP64 stays bit-identical."""
+    monkeypatch.setenv("SPARKLE_MIXED_VARIANT", str(variant))
+    cx = sd.SyntheticComplex(757, 481, 1, 64, seed=61)
+    poses = cx.poses.reshape(-1, cx.pose_len).copy()[:64]
+    rng = np.random.default_rng(5)
+    poses[:, 7:] *= rng.uniform(1.0, 150.0, size=(len(poses), 1))  # displacement bounds up to ~120 A
+    _, ref_en = oracle_scores(OracleSystem(cx, tables), poses)
+    with sd.Docking([cx], tables, precision=sd.SD_PREC_MIXED) as dk:
+        dk.init_state(0, cx.poses)
+        dk.set_draws(0, sd.gso_draws(0, cx.n_swarms, 1, cx.n_glowworms))
+        dk.step(1)
+        assert dk.tuning()["variant"] == variant
+        _, en = dk.score_poses(0, poses, sd.SD_PREC_MIXED)
+        assert rel_err(en, ref_en).max() <= MIXED_TOL
+        _, en64 = dk.score_poses(0, poses, sd.SD_PREC_FP64)
+        assert np.array_equal(en64, ref_en)
