@@ -168,6 +168,39 @@ int sd_get_stats(sd_ctx* ctx, sd_stats* out);
  * context before its first mixed step; SPARKLE_TUNE=0 disables it, SPARKLE_MIXED_VARIANT=k
  * forces a variant. */
 int sd_get_tuning(sd_ctx* ctx, int* variant, int* warps, int* min_blocks, double* ms, int n_ms);
+/* ---- Structures from PDB files (the setup stage in front of the GSO path) ----
+ * Reads the first structure of a PDB file as the reference's setup does (read_input_structure,
+ * source/prep/src/read_input_structure.cc:60-307; generate_complex, source/prep/src/complex.cc;
+ * init_center_translate + translate, source/prep/src/initialization.cc:3-29; get_nm_mask,
+ * complex.cc:143-209; get_docking_model, source/dock/src/prepare_gso_tasks.cc:31-69): atoms of
+ * the first MODEL, coordinates through float, centred on the mean of the non-hydrogen atoms, the
+ * normal-mode mask (protein and nucleic residues), the DFIRE atom type of every atom and a
+ * backbone flag (CA or P).  Errors: unreadable file, no atoms, unrecognised element, atom without
+ * a DFIRE type. */
+typedef struct sd_structure sd_structure;
+#define SD_PDB_NOXT 1 /* ignore OXT atoms (setup.json "noxt") */
+#define SD_PDB_NOH 2  /* ignore hydrogens ("noh") */
+#define SD_PDB_NOW 4  /* ignore waters, HOH ("now") */
+int sd_structure_load(const char* pdb_path, int flags, sd_structure** out);
+int sd_structure_info(const sd_structure* s, int* n_atoms, int* n_residues);
+/* Any output may be NULL: xyz [n][3] (centred), nm_mask [n], dfire_type [n], backbone [n],
+ * translation [3] (the vector added to the file's coordinates). */
+int sd_structure_arrays(const sd_structure* s, double* xyz, int* nm_mask, int* dfire_type, int* backbone,
+                        double* translation);
+int sd_structure_free(sd_structure* s);
+
+/* Khachiyan minimum-volume enclosing ellipsoid centre of n points (tolerance 0.01), the ligand
+ * reference point of minimum_volume_ellipsoid (source/dock/src/prepare_gso_tasks.cc:106-267). */
+int sd_reference_point(const double* xyz, int n, double* center);
+/* Seeded starting poses [n_swarms][n_glowworms][pose_len] around a receptor centred at the
+ * origin: swarm centres at uniform directions on a shell 10 A outside its bounding sphere, each
+ * glowworm at its centre plus N(0, 2 A) per axis, a uniform random unit quaternion and N(0, 1)
+ * ANM extents.  A stand-in for the reference's surface-based swarm placement
+ * (calculate_start_pos, source/prep/src/initialization.cc), which is a setup stage not built
+ * here. */
+int sd_starting_poses(const double* rec_xyz, int n_rec, int n_swarms, int n_glowworms, int n_modes_rec,
+                      int n_modes_lig, unsigned long long seed, double* poses);
+
 /* Number of compiled variants of the mixed-precision DFIRE kernel (valid SPARKLE_MIXED_VARIANT
  * values are 0 .. count-1; sd_get_tuning reports one time per variant). */
 int sd_mixed_variant_count(void);

@@ -22,6 +22,9 @@
 
 #include "complex.h"
 #include "fastdfire.h"
+#include "initialization.h"
+#include "read_input_structure.h"
+#include "translate.h"
 #include "prepare_gso_tasks.h"
 #include "swarm_centers.h"
 
@@ -282,6 +285,35 @@ int ref_run_cal_gso_tasks_cpu(const or_system* s, const double* pos0, int nthrea
   int status = 0;
   waitpid(pid, &status, 0);
   return WIFEXITED(status) ? WEXITSTATUS(status) : -1;
+}
+
+// The reference's own setup chain for one structure, as run_simulation.cc:53-79 and
+// prepare_gso_tasks.cc:1177-1188 run it: read_input_structure, init_center_translate, translate,
+// get_nm_mask, get_docking_model.  Copies out up to cap atoms; returns the atom count (or -1).
+int ref_load_structure(const char* path, int noxt, int noh, int now, double* xyz, int* mask, int* dfire,
+                       double* translation, int cap) {
+  Complex c;
+  read_input_structure(c, path, noxt != 0, noh != 0, now != 0, false, (int)strlen(path));
+  init_center_translate(c.translation, c.atom_coordinates, c.elements, c.structure_size, c.num_atoms,
+                        c.num_structures);
+  translate(c.atom_coordinates, c.translation, c.structure_size, c.num_atoms, c.num_structures);
+  get_nm_mask(c.mask, c.residue_name, c.STANDARD_TYPES, c.MODIFIED_TYPES, c.DNA_STANDARD_TYPES,
+              c.RNA_STANDARD_TYPES, c.residue_atom_number, c.residue_size);
+  FastDifire fd;
+  const int nobj = (int)c.chain.size() * c.residue_atom_number[c.num_res_type];
+  int* objs = new int[nobj > 0 ? nobj : 1];
+  get_docking_model(objs, c, fd);
+  const int n = c.num_atoms;
+  if (n > cap) {
+    delete[] objs;
+    return -1;
+  }
+  memcpy(xyz, c.atom_coordinates, sizeof(double) * 3 * n);
+  memcpy(mask, c.mask, sizeof(int) * n);
+  memcpy(dfire, objs, sizeof(int) * n);
+  memcpy(translation, c.translation, sizeof(double) * 3);
+  delete[] objs;
+  return n;
 }
 
 }  // extern "C"

@@ -13,10 +13,10 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _abi
-from ._abi import (SD_PREC_FP64, SD_PREC_FP64_REF, SD_PREC_MIXED, SD_SCORING_DFIRE,  # noqa: F401
-                   SD_SCORING_PYDOCK, SparkleError, check, dptr, iptr)
+from ._abi import (SD_PDB_NOH, SD_PDB_NOW, SD_PDB_NOXT, SD_PREC_FP64, SD_PREC_FP64_REF,  # noqa: F401
+                   SD_PREC_MIXED, SD_SCORING_DFIRE, SD_SCORING_PYDOCK, SparkleError, check, dptr, iptr)
 
-__all__ = ["SyntheticComplex", "synthetic_tables", "gso_draws", "mixed_variant_count", "GsoParams", "Docking",
+__all__ = ["SyntheticComplex", "Structure", "synthetic_tables", "gso_draws", "mixed_variant_count", "GsoParams", "Docking",
            "SD_PREC_FP64_REF", "SD_PREC_FP64", "SD_PREC_MIXED", "SD_SCORING_DFIRE",
            "SD_SCORING_PYDOCK", "SparkleError", "device_count"]
 
@@ -90,6 +90,29 @@ class SyntheticComplex:
         self.lig_lj = view(d.lig_lj_type, (n_lig,), np.int32)
         self.lig_ref = np.array(list(d.lig_ref_point), np.float64)
         self.poses = view(poses, (n_swarms, n_glowworms, self.pose_len), np.float64)
+
+
+class Structure:
+    """A structure read from a PDB file as the reference's setup reads it (first MODEL, centred
+    coordinates, normal-mode mask, DFIRE atom types, CA/P backbone flags); flags are
+    SD_PDB_NOXT | SD_PDB_NOH | SD_PDB_NOW (setup.json noxt / noh / now)."""
+
+    def __init__(self, path: str, flags: int = 0):
+        h = C.c_void_p()
+        check(_abi.lib().sd_structure_load(str(path).encode(), flags, C.byref(h)), "sd_structure_load")
+        try:
+            n, nr = C.c_int(), C.c_int()
+            check(_abi.lib().sd_structure_info(h, C.byref(n), C.byref(nr)), "sd_structure_info")
+            self.n_atoms, self.n_residues = n.value, nr.value
+            self.xyz = np.empty((self.n_atoms, 3))
+            self.nm_mask = np.empty(self.n_atoms, np.int32)
+            self.dfire_type = np.empty(self.n_atoms, np.int32)
+            self.backbone = np.empty(self.n_atoms, np.int32)
+            self.translation = np.empty(3)
+            check(_abi.lib().sd_structure_arrays(h, dptr(self.xyz), iptr(self.nm_mask), iptr(self.dfire_type),
+                                                 iptr(self.backbone), dptr(self.translation)), "sd_structure_arrays")
+        finally:
+            _abi.lib().sd_structure_free(h)
 
 
 def GsoParams(**kw) -> _abi.GsoParams:

@@ -17,6 +17,7 @@ SD_OK, SD_ERR_ARG, SD_ERR_OOM, SD_ERR_CUDA, SD_ERR_TIMEOUT, SD_ERR_NUMERIC, SD_E
 SD_DFIRE_TYPES, SD_DFIRE_BINS, SD_MAX_MODES, SD_LJ_TYPES = 168, 20, 10, 20
 SD_SCORING_DFIRE, SD_SCORING_PYDOCK = 0, 1
 SD_PREC_FP64_REF, SD_PREC_FP64, SD_PREC_MIXED = 0, 1, 2
+SD_PDB_NOXT, SD_PDB_NOH, SD_PDB_NOW = 1, 2, 4
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -91,6 +92,12 @@ SIGNATURES = {
     "sd_get_stats": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     "sd_get_tuning": (C.c_int, [C.c_void_p, _ip, _ip, _ip, _dp, C.c_int]),
     "sd_mixed_variant_count": (C.c_int, []),
+    "sd_structure_load": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "sd_reference_point": (C.c_int, [_dp, C.c_int, _dp]),
+    "sd_starting_poses": (C.c_int, [_dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_ulonglong, _dp]),
+    "sd_structure_info": (C.c_int, [C.c_void_p, _ip, _ip]),
+    "sd_structure_arrays": (C.c_int, [C.c_void_p, _dp, _ip, _ip, _ip, _dp]),
+    "sd_structure_free": (C.c_int, [C.c_void_p]),
     "sd_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
     "sd_score_poses": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_int, C.c_int, _dp, _dp]),
     "sd_score_poses_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p,

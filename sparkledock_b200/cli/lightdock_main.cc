@@ -9,13 +9,18 @@
 //   "scoring": "dfire" | "pydock"                (absent: dfire)
 //   "precision": "mixed" | "fp64" | "fp64_ref"  (absent: mixed)
 //   "translation_step", "rotation_step", "nmodes_step"   (absent: the reference's 0.5)
+//   receptor_pdb, ligand_pdb, noxt, noh, now: the structures, read as the reference's setup
+//        reads them (sd_structure_load); ANM modes and pyDock charges are seeded stand-ins and
+//        the starting poses come from sd_starting_poses (ANM, charges and the reference's
+//        surface-based swarm placement are setup stages not built here)
 //   "synthetic": {"receptor_atoms": N, "ligand_atoms": M, "seed": s}
-//        seeded synthetic receptor/ligand in place of receptor_pdb / ligand_pdb (PDB parsing,
-//        ANM and swarm placement are setup stages outside this path)
+//        seeded synthetic receptor/ligand in place of receptor_pdb / ligand_pdb
 //   "dfire_table": path of a DCparams-format file (168*168*20 values, one per line);
 //        absent: seeded synthetic table ("table_seed", default 3)
 // -s STEPS is honoured (the reference parses it but runs its compiled STEPS macro).
 // Output: <dir>/swarm_<i>/gso_<STEPS>.out as the reference GPU path writes them.
+#include <errno.h>
+#include <sys/stat.h>
 #include <unistd.h>
 
 #include <chrono>
@@ -217,24 +222,63 @@ int main(int argc, char** argv) {
   int precision = prec_s == "mixed" ? SD_PREC_MIXED : prec_s == "fp64" ? SD_PREC_FP64 : prec_s == "fp64_ref" ? SD_PREC_FP64_REF : -1;
   if (precision < 0) return die("setup.json: \"precision\" must be \"mixed\", \"fp64\" or \"fp64_ref\"");
   const JVal* syn = root.get("synthetic");
-  if (!syn || syn->kind != JVal::Obj)
-    return die("setup.json: PDB inputs (receptor_pdb / ligand_pdb) need the setup stages (PDB parsing, ANM, "
-               "swarm placement) that this path does not include; give a \"synthetic\" block");
+  const bool pdb_input = !syn || syn->kind != JVal::Obj;
+  // PDB inputs: structures read as the reference's setup reads them (flags noxt / noh / now)
+  std::unique_ptr<sd_structure, int (*)(sd_structure*)> rec_s(nullptr, sd_structure_free),
+      lig_s(nullptr, sd_structure_free);
+  if (pdb_input) {
+    const std::string rp = str_or(root, "receptor_pdb", ""), lp = str_or(root, "ligand_pdb", "");
+    if (rp.empty() || lp.empty())
+      return die("setup.json: give receptor_pdb and ligand_pdb, or a \"synthetic\" block");
+    auto flag = [&](const char* k) {
+      const JVal* v = root.get(k);
+      return v && v->kind == JVal::Bool && v->b;
+    };
+    const int fl = (flag("noxt") ? SD_PDB_NOXT : 0) | (flag("noh") ? SD_PDB_NOH : 0) | (flag("now") ? SD_PDB_NOW : 0);
+    auto resolve = [&](const std::string& f) {  // as given, else next to setup.json
+      if (std::ifstream(f).good() || f.empty() || f[0] == '/') return f;
+      const size_t sl = file.rfind('/');
+      return sl == std::string::npos ? f : file.substr(0, sl + 1) + f;
+    };
+    sd_structure* a = nullptr;
+    sd_structure* b = nullptr;
+    if (sd_structure_load(resolve(rp).c_str(), fl, &a) != SD_OK) return die(sd_last_error());
+    rec_s.reset(a);
+    if (sd_structure_load(resolve(lp).c_str(), fl, &b) != SD_OK) return die(sd_last_error());
+    lig_s.reset(b);
+  }
 
   sd_synth_spec spec;
-  spec.n_rec = (int)num_or(*syn, "receptor_atoms", 0);
-  spec.n_lig = (int)num_or(*syn, "ligand_atoms", 0);
   spec.n_swarms = swarms;
   spec.n_glowworms = G;
   spec.n_modes_rec = anm_rec;
   spec.n_modes_lig = anm_lig;
-  spec.seed = (unsigned long long)num_or(*syn, "seed", num_or(root, "starting_points_seed", 1));
+  spec.seed = (unsigned long long)num_or(pdb_input ? root : *syn, "seed", num_or(root, "starting_points_seed", 1));
+  if (pdb_input) {
+    sd_structure_info(rec_s.get(), &spec.n_rec, nullptr);
+    sd_structure_info(lig_s.get(), &spec.n_lig, nullptr);
+  } else {
+    spec.n_rec = (int)num_or(*syn, "receptor_atoms", 0);
+    spec.n_lig = (int)num_or(*syn, "ligand_atoms", 0);
+  }
   long long bytes = 0;
   if (sd_synth_buffer_size(&spec, &bytes) != SD_OK) return die(sd_last_error());
   std::unique_ptr<char[]> buf(new char[(size_t)bytes]);
   sd_complex_desc desc;
   double* pos0 = nullptr;
   if (sd_synth_generate(&spec, buf.get(), &desc, &pos0) != SD_OK) return die(sd_last_error());
+  if (pdb_input) {
+    // real coordinates, masks and DFIRE types; ANM modes and pyDock charges / LJ types stay the
+    // seeded stand-ins (ANM and charge assignment are setup stages not built here); reference
+    // point and starting poses from the real structures
+    sd_structure_arrays(rec_s.get(), const_cast<double*>(desc.rec_xyz), const_cast<int*>(desc.rec_mask),
+                        const_cast<int*>(desc.rec_dfire_type), nullptr, nullptr);
+    sd_structure_arrays(lig_s.get(), const_cast<double*>(desc.lig_xyz), const_cast<int*>(desc.lig_mask),
+                        const_cast<int*>(desc.lig_dfire_type), nullptr, nullptr);
+    if (sd_reference_point(desc.lig_xyz, desc.n_lig, desc.lig_ref_point) != SD_OK) return die(sd_last_error());
+    if (sd_starting_poses(desc.rec_xyz, desc.n_rec, swarms, G, anm_rec, anm_lig, spec.seed, pos0) != SD_OK)
+      return die(sd_last_error());
+  }
 
   const size_t tsz = (size_t)SD_DFIRE_TYPES * SD_DFIRE_TYPES * SD_DFIRE_BINS;
   std::vector<double> table(tsz), eps(SD_LJ_TYPES), sig(SD_LJ_TYPES);
@@ -277,15 +321,21 @@ int main(int argc, char** argv) {
   sd_swarm_state st = {pos.data(), sc.data(), luc.data(), vis.data(), nullptr, nullptr, nnei.data(), nullptr, nullptr};
   if (!rc) rc = sd_get_state(ctx, 0, &st);
   const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  sd_stats stats = {};
+  if (!rc) rc = sd_get_stats(ctx, &stats);
   if (rc) {
     const std::string m = sd_last_error();
     sd_ctx_destroy(ctx);
     return die(m);
   }
   sd_ctx_destroy(ctx);
+  if (!outdir.empty() && outdir != "." && mkdir(outdir.c_str(), 0755) != 0 && errno != EEXIST)
+    return die("cannot create output directory " + outdir);
   if (sd_write_gso_output(outdir.c_str(), 0, swarms, G, pl, steps, pos.data(), luc.data(), nnei.data(), vis.data(),
                           sc.data()) != SD_OK)
     return die(sd_last_error());
   printf("simulation execution:%f\n", secs);
+  printf("scored poses: %lld (%.0f per second, wall clock including setup and state transfers)\n",
+         stats.scored_poses, stats.scored_poses / secs);
   return 0;
 }

@@ -107,6 +107,41 @@ void atoms(Rng& r, int n, int* type, double* charge, int* lj, int* mask) {
 // Khachiyan's minimum-volume enclosing ellipsoid centre (the ligand reference point of
 // prepare_gso_tasks.cc:106-267 / :1196-1202, tolerance 0.01 as at :1196).  Only the diagonal
 // q_i^T X^-1 q_i is formed, O(N) per iteration.
+// Starting poses: swarm centres at independent uniform directions on a shell 10 A outside the
+// receptor's bounding sphere (receptor centred at the origin), each glowworm at its centre plus
+// N(0, 2 A) per axis, a uniform random unit quaternion (Shoemake) and N(0, 1) ANM extents.
+void starting_poses(Rng& rs, const double* rec_xyz, int n_rec, int S, int G, int nmr, int nml, double* poses) {
+  double rmax = 0;
+  for (int i = 0; i < n_rec; ++i)
+    rmax = std::max(rmax, std::sqrt(rec_xyz[i * 3] * rec_xyz[i * 3] + rec_xyz[i * 3 + 1] * rec_xyz[i * 3 + 1] +
+                                    rec_xyz[i * 3 + 2] * rec_xyz[i * 3 + 2]));
+  const double shell = rmax + 10.0;
+  const int pl = SD_POSE_LEN(nmr, nml);
+  const double PI = 3.14159265358979323846;
+  for (int sw = 0; sw < S; ++sw) {
+    double v[3], n2 = 0;
+    do {
+      n2 = 0;
+      for (int k = 0; k < 3; ++k) {
+        v[k] = rs.normal();
+        n2 += v[k] * v[k];
+      }
+    } while (n2 < 1e-12);
+    double nrm = std::sqrt(n2);
+    double c[3] = {v[0] / nrm * shell, v[1] / nrm * shell, v[2] / nrm * shell};
+    for (int g = 0; g < G; ++g) {
+      double* p = poses + ((size_t)sw * G + g) * pl;
+      for (int k = 0; k < 3; ++k) p[k] = c[k] + 2.0 * rs.normal();
+      double u1 = rs.uniform(), u2 = rs.uniform(), u3 = rs.uniform();
+      p[3] = std::sqrt(1 - u1) * std::sin(2 * PI * u2);
+      p[4] = std::sqrt(1 - u1) * std::cos(2 * PI * u2);
+      p[5] = std::sqrt(u1) * std::sin(2 * PI * u3);
+      p[6] = std::sqrt(u1) * std::cos(2 * PI * u3);
+      for (int k = 0; k < nmr + nml; ++k) p[7 + k] = rs.normal();
+    }
+  }
+}
+
 void mvee_center(const double* p, int n, double tol, double* center) {
   std::vector<double> u(n, 1.0 / n);
   double err = 1 + tol;
@@ -255,37 +290,24 @@ extern "C" int sd_synth_generate(const sd_synth_spec* s, void* buf, sd_complex_d
   d->n_swarms = s->n_swarms;
   d->n_glowworms = s->n_glowworms;
 
-  // swarm centres on a shell 10 A outside the receptor surface
-  double rmax = 0;
-  for (int i = 0; i < s->n_rec; ++i)
-    rmax = std::max(rmax, std::sqrt(rec_xyz[i * 3] * rec_xyz[i * 3] + rec_xyz[i * 3 + 1] * rec_xyz[i * 3 + 1] +
-                                    rec_xyz[i * 3 + 2] * rec_xyz[i * 3 + 2]));
-  const double shell = rmax + 10.0;
-  const int pl = SD_POSE_LEN(s->n_modes_rec, s->n_modes_lig);
-  const double PI = 3.14159265358979323846;
-  for (int sw = 0; sw < s->n_swarms; ++sw) {
-    double v[3], n2 = 0;
-    do {
-      n2 = 0;
-      for (int k = 0; k < 3; ++k) {
-        v[k] = rs.normal();
-        n2 += v[k] * v[k];
-      }
-    } while (n2 < 1e-12);
-    double nrm = std::sqrt(n2);
-    double c[3] = {v[0] / nrm * shell, v[1] / nrm * shell, v[2] / nrm * shell};
-    for (int g = 0; g < s->n_glowworms; ++g) {
-      double* p = poses + ((size_t)sw * s->n_glowworms + g) * pl;
-      for (int k = 0; k < 3; ++k) p[k] = c[k] + 2.0 * rs.normal();
-      double u1 = rs.uniform(), u2 = rs.uniform(), u3 = rs.uniform();
-      p[3] = std::sqrt(1 - u1) * std::sin(2 * PI * u2);
-      p[4] = std::sqrt(1 - u1) * std::cos(2 * PI * u2);
-      p[5] = std::sqrt(u1) * std::sin(2 * PI * u3);
-      p[6] = std::sqrt(u1) * std::cos(2 * PI * u3);
-      for (int k = 0; k < s->n_modes_rec + s->n_modes_lig; ++k) p[7 + k] = rs.normal();
-    }
-  }
+  sd::starting_poses(rs, rec_xyz, s->n_rec, s->n_swarms, s->n_glowworms, s->n_modes_rec, s->n_modes_lig, poses);
   if (poses_out) *poses_out = poses;
+  return SD_OK;
+}
+
+extern "C" int sd_starting_poses(const double* rec_xyz, int n_rec, int n_swarms, int n_glowworms, int n_modes_rec,
+                                 int n_modes_lig, unsigned long long seed, double* poses) {
+  if (!rec_xyz || !poses || n_rec <= 0 || n_swarms <= 0 || n_glowworms <= 0 || n_modes_rec < 0 ||
+      n_modes_rec > SD_MAX_MODES || n_modes_lig < 0 || n_modes_lig > SD_MAX_MODES)
+    return sd::fail(SD_ERR_ARG, "sd_starting_poses: bad arguments");
+  sd::Rng rs(seed * 4 + 3);
+  sd::starting_poses(rs, rec_xyz, n_rec, n_swarms, n_glowworms, n_modes_rec, n_modes_lig, poses);
+  return SD_OK;
+}
+
+extern "C" int sd_reference_point(const double* xyz, int n, double* center) {
+  if (!xyz || n <= 0 || !center) return sd::fail(SD_ERR_ARG, "sd_reference_point: bad arguments");
+  sd::mvee_center(xyz, n, 0.01, center);
   return SD_OK;
 }
 

@@ -92,6 +92,8 @@ def ref():
         L.ref_gso_step.argtypes = [C.POINTER(OrSystem), C.POINTER(OrState), _dp, C.c_int]
         L.ref_slerp.argtypes = [_dp, _dp, C.c_double]
         L.ref_min_volume_ellipsoid.argtypes = [_dp, C.c_int, _dp, _dp]
+        L.ref_load_structure.restype = C.c_int
+        L.ref_load_structure.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, _dp, _ip, _ip, _dp, C.c_int]
         L.ref_run_cal_gso_tasks_cpu.restype = C.c_int
         L.ref_run_cal_gso_tasks_cpu.argtypes = [C.POINTER(OrSystem), _dp, C.c_int, C.c_char_p, C.c_int]
         _ref = L
@@ -200,3 +202,16 @@ def oracle_bins(osys: OracleSystem, pose: np.ndarray):
     ref = np.zeros(3)
     sc = oracle().or_score_pose(osys.ptr, _d(pose), C.byref(e), _d(ref), _i(bins), C.byref(cnt))
     return bins, sc, e.value, ref, cnt
+
+
+def ref_structure(path: str, noxt: bool, noh: bool, now: bool, cap: int = 40000):
+    """The reference's own setup of one structure (compiled from its sources): centred
+    coordinates, normal-mode mask, DFIRE types, translation."""
+    xyz = np.empty((cap, 3))
+    mask = np.empty(cap, np.int32)
+    dfire = np.empty(cap, np.int32)
+    tr = np.empty(3)
+    n = ref().ref_load_structure(str(path).encode(), int(noxt), int(noh), int(now), _d(xyz), _i(mask), _i(dfire),
+                                 _d(tr), cap)
+    assert n >= 0
+    return xyz[:n].copy(), mask[:n].copy(), dfire[:n].copy(), tr

@@ -29,7 +29,11 @@ def test_cli_usage_and_setup_errors(tmp_path):
     pdb = tmp_path / "pdb.json"
     pdb.write_text(json.dumps({"swarms": 2, "receptor_pdb": "r.pdb", "ligand_pdb": "l.pdb"}))
     r = run(["-f", str(pdb)])
-    assert r.returncode != 0 and "synthetic" in r.stderr
+    assert r.returncode != 0 and "cannot open" in r.stderr
+    nopdb = tmp_path / "nopdb.json"
+    nopdb.write_text(json.dumps({"swarms": 2}))
+    r = run(["-f", str(nopdb)])
+    assert r.returncode != 0 and "receptor_pdb" in r.stderr
     sc = tmp_path / "sc.json"
     sc.write_text(json.dumps({"swarms": 2, "scoring": "vina", "synthetic": {"receptor_atoms": 50, "ligand_atoms": 40}}))
     r = run(["-f", str(sc)])
@@ -67,3 +71,54 @@ def test_cli_fp64_run_matches_oracle(tmp_path, tables):
     for s in range(2):
         got = (tmp_path / f"swarm_{s}" / f"gso_{steps}.out").read_text()
         assert got == exp[s]
+
+
+def write_pdb(path, xyz, chain):
+    """A PDB of glycines (N, CA, C, O per residue) at the given coordinates (4 atoms per residue)."""
+    names = ("N", "CA", "C", "O")
+    with open(path, "w") as f:
+        for i, (x, y, z) in enumerate(xyz):
+            f.write("ATOM  %5d  %-3s GLY %s%4d    %8.3f%8.3f%8.3f  1.00  0.00\n" % (i + 1, names[i % 4], chain,
+                                                                              i // 4 + 1, x, y, z))
+        f.write("END\n")
+
+
+@pytest.mark.gpu
+def test_cli_pdb_inputs_match_oracle(tmp_path, tables):
+    """PDB inputs through the command line: structures read as the reference's setup reads them,
+    seeded ANM modes, reference point and starting poses from the real coordinates; the FP64 run's
+    output files equal the oracle's trajectory on the same complex."""
+    rec0 = sd.SyntheticComplex(400, 248, 1, 4, seed=31)
+    write_pdb(tmp_path / "rec.pdb", rec0.rec_xyz + 20.0, "A")
+    write_pdb(tmp_path / "lig.pdb", rec0.lig_xyz - 7.0, "B")
+    seed, S, G, steps = 19, 2, 40, 6
+    setup = {"swarms": S, "glowworms": G, "anm_rec": 10, "anm_lig": 10, "use_anm": True, "precision": "fp64",
+             "scoring": "dfire", "receptor_pdb": "rec.pdb", "ligand_pdb": "lig.pdb", "noxt": True, "noh": True,
+             "now": True, "starting_points_seed": seed}
+    (tmp_path / "setup.json").write_text(json.dumps(setup))
+    r = run(["-f", "setup.json", "-s", str(steps)], cwd=tmp_path)
+    assert r.returncode == 0, r.stderr
+    # the same complex built through the Python view of the ABI
+    rs = sd.Structure(str(tmp_path / "rec.pdb"), sd.SD_PDB_NOXT | sd.SD_PDB_NOH | sd.SD_PDB_NOW)
+    ls = sd.Structure(str(tmp_path / "lig.pdb"), sd.SD_PDB_NOXT | sd.SD_PDB_NOH | sd.SD_PDB_NOW)
+    cx = sd.SyntheticComplex(rs.n_atoms, ls.n_atoms, S, G, 10, 10, seed=seed)
+    cx.rec_xyz[:] = rs.xyz
+    cx.rec_mask[:] = rs.nm_mask
+    cx.rec_type[:] = rs.dfire_type
+    cx.lig_xyz[:] = ls.xyz
+    cx.lig_mask[:] = ls.nm_mask
+    cx.lig_type[:] = ls.dfire_type
+    ref = np.empty(3)
+    sd._abi.lib().sd_reference_point(sd.dptr(cx.lig_xyz), ls.n_atoms, sd.dptr(ref))
+    cx.lig_ref = ref
+    poses = np.empty_like(cx.poses)
+    sd._abi.lib().sd_starting_poses(sd.dptr(cx.rec_xyz), rs.n_atoms, S, G, 10, 10, seed, sd.dptr(poses))
+    osys = OracleSystem(cx, tables)
+    st = OracleState(S, G, cx.pose_len, poses)
+    U = sd.gso_draws(0, S, steps, G)
+    for t in range(steps):
+        oracle_step(osys, st, U[:, t, :])
+    exp = gso_lines(st, cx.pose_len)
+    for sw in range(S):
+        got = (tmp_path / f"swarm_{sw}" / f"gso_{steps}.out").read_text()
+        assert got == exp[sw]
