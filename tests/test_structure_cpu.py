@@ -114,3 +114,22 @@ def test_starting_poses_match_synthetic_generator():
     ref = np.empty(3)
     assert sd._abi.lib().sd_reference_point(sd.dptr(cx.lig_xyz), 200, sd.dptr(ref)) == 0
     assert np.array_equal(ref, cx.lig_ref)
+
+
+@needs_ref
+def test_reference_point_matches_reference_ellipsoid():
+    """sd_reference_point (Khachiyan MVEE centre, tolerance 0.01) against the reference's own
+    minimum_volume_ellipsoid: within 1e-12 (the iteration is restated with its own linear algebra,
+    not Eigen's, so the last bits may differ) on random point clouds and the shipped ligands."""
+    import ctypes as C
+    from oracle_bind import ref
+    dp = C.POINTER(C.c_double)
+    rng = np.random.default_rng(0)
+    clouds = [np.ascontiguousarray(rng.normal(size=(int(rng.integers(50, 1500)), 3)) * rng.uniform(5, 20, 3))
+              for _ in range(10)]
+    clouds += [sd.Structure(p, sd.SD_PDB_NOXT | sd.SD_PDB_NOH | sd.SD_PDB_NOW).xyz for p in PDBS if "_l_" in p]
+    for pts in clouds:
+        a, c, poles = np.empty(3), np.empty(3), np.empty(18)
+        assert sd._abi.lib().sd_reference_point(sd.dptr(pts), len(pts), sd.dptr(a)) == 0
+        ref().ref_min_volume_ellipsoid(pts.ctypes.data_as(dp), len(pts), c.ctypes.data_as(dp), poles.ctypes.data_as(dp))
+        assert np.abs(a - c).max() <= 1e-12 * max(1.0, np.abs(c).max())
