@@ -144,6 +144,20 @@ def run_gpu(cfg, prec_name, steps, warmup, device, flush, seed=0, per_step=False
     return out
 
 
+def time_clustering(dk, cxs):
+    """Wall clock of one sd_cluster call on the final poses of the first complex (every swarm),
+    backbone = every 8th atom (about one CA per residue of a protein)."""
+    c = cxs[0]
+    rb = (np.arange(c.n_rec) % 8 == 1).astype(np.int32)
+    lb = (np.arange(c.n_lig) % 8 == 1).astype(np.int32)
+    dk.cluster(0, rb, lb)
+    t0 = time.perf_counter()
+    out = dk.cluster(0, rb, lb)
+    dt = time.perf_counter() - t0
+    return {"ms": dt * 1e3, "swarms": c.n_swarms, "glowworms": c.n_glowworms,
+            "backbone_atoms": int(rb.sum() + lb.sum()), "mean_clusters_per_swarm": float(out["n_clusters"].mean())}
+
+
 def fp64_spot_check(dk, cxs, frac=0.01):
     """Energies of 1 % of the final poses (at least 256 per complex) from the mixed kernel
     against the plain FP64 kernel: max |E_mixed - E_fp64| / max(|E_fp64|, 1) on the raw DFIRE
@@ -385,6 +399,7 @@ def main():
     pairs_timed_rank = run["pairs"]
     tuning = run["tuning"]
     spot = fp64_spot_check(run["ctx"], run["cxs"]) if cfg["precision"] == "mixed" else None
+    clustering = time_clustering(run["ctx"], run["cxs"])
     run["ctx"].close()
 
     extra = {}
@@ -434,6 +449,7 @@ def main():
         "mixed_vs_fp64": extra,
         "autotuner": tuning,
         "fp64_spot_check": spot,
+        "final_clustering": clustering,
         **({"per_step": {"scored_poses": run["per_step"], "ms": run["ms"]}} if args.per_step else {}),
         "edge_counts": {k: stats[k] for k in ("pairs_fallback", "edge_d2_zero", "edge_d2_cutoff", "edge_u_zero",
                                               "edge_shortfall")},

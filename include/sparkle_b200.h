@@ -201,6 +201,23 @@ int sd_reference_point(const double* xyz, int n, double* center);
 int sd_starting_poses(const double* rec_xyz, int n_rec, int n_swarms, int n_glowworms, int n_modes_rec,
                       int n_modes_lig, unsigned long long seed, double* poses);
 
+/* Final-pose clustering of every swarm of complex ci (BSAS, as the reference's GPU pipeline
+ * variant clusters before writing cluster.repr, source/dock/src/cuda/pipeline:2766-2960):
+ * glowworms ordered by score (descending; key (int64)(score * 2^50) / 2^12 * 2^12 + index), each
+ * joins the first cluster whose representative (first member) is within 4 A backbone RMSD, else
+ * starts a new cluster.  Backbone RMSD over the flagged atoms (rec_backbone [n_rec],
+ * lig_backbone [n_lig], e.g. sd_structure_arrays' CA / P flags) of the final poses, receptor
+ * then ligand, no superposition.  As in the reference, the first glowworm in score order is
+ * compared with its own cluster again, so cluster 0's size counts it twice.  Outputs:
+ * n_clusters [S]; cluster_rep, cluster_len [S][G] (first n_clusters[s] entries of each swarm are
+ * used); member_of [S][G] (cluster of each glowworm). */
+int sd_cluster(sd_ctx* ctx, int ci, const int* rec_backbone, const int* lig_backbone, int* n_clusters,
+               int* cluster_rep, int* cluster_len, int* member_of);
+/* <dir>/swarm_<offset+s>/cluster.repr for n_swarms swarms from sd_cluster's outputs and the
+ * swarms' scores [S][G] ("<c>:<size>:<score>:<rep>:lightdock_<rep>.pdb" per cluster). */
+int sd_write_cluster_repr(const char* dir, int swarm_offset, int n_swarms, int n_glowworms, const int* n_clusters,
+                          const int* cluster_rep, const int* cluster_len, const double* scoring);
+
 /* Number of compiled variants of the mixed-precision DFIRE kernel (valid SPARKLE_MIXED_VARIANT
  * values are 0 .. count-1; sd_get_tuning reports one time per variant). */
 int sd_mixed_variant_count(void);

@@ -646,3 +646,75 @@ void or_key_thresholds(double* t) {
     t[m] = hi;
   }
 }
+
+/* ---------------------------------------------------------------------------------------
+ * Final-pose clustering (pipeline:2766-2960).  Key: (int64)(score * 2^50) / 2^12 * 2^12 + g,
+ * sorted descending; cluster 0 starts with the first glowworm, then every glowworm in order
+ * (the first again) joins the first cluster whose representative is within 4 A RMSD over the
+ * flagged atoms (per atom ((0 + dx^2) + dy^2) + dz^2 added in order, receptor then ligand,
+ * divided by the count, square root), else starts a new cluster.
+ * ------------------------------------------------------------------------------------- */
+void or_cluster(const or_system* sys, const double* pos, const double* scores, const int* rec_bb,
+                const int* lig_bb, int* n_clusters, int* rep, int* size, int* member) {
+  const int S = sys->S, G = sys->G, nr = sys->nr, nl = sys->nl, pl = 7 + sys->nmr + sys->nml;
+  int nbb = 0;
+  for (int i = 0; i < nr; ++i) nbb += rec_bb[i] != 0;
+  for (int j = 0; j < nl; ++j) nbb += lig_bb[j] != 0;
+  double* rec = (double*)malloc(sizeof(double) * 3 * nr);
+  double* lig = (double*)malloc(sizeof(double) * 3 * nl);
+  double* bb = (double*)malloc(sizeof(double) * 3 * (size_t)nbb * G);
+  long long* key = (long long*)malloc(sizeof(long long) * G);
+  int* order = (int*)malloc(sizeof(int) * G);
+  for (int s = 0; s < S; ++s) {
+    for (int g = 0; g < G; ++g) {
+      const double* p = pos + ((size_t)s * G + g) * pl;
+      double refp[3];
+      or_receptor_pose(sys, p, rec);
+      or_ligand_pose(sys, p, lig, refp);
+      double* o = bb + (size_t)g * nbb * 3;
+      int k = 0;
+      for (int i = 0; i < nr; ++i)
+        if (rec_bb[i]) { o[k * 3] = rec[i * 3]; o[k * 3 + 1] = rec[i * 3 + 1]; o[k * 3 + 2] = rec[i * 3 + 2]; ++k; }
+      for (int j = 0; j < nl; ++j)
+        if (lig_bb[j]) { o[k * 3] = lig[j * 3]; o[k * 3 + 1] = lig[j * 3 + 1]; o[k * 3 + 2] = lig[j * 3 + 2]; ++k; }
+      double sc = scores[(size_t)s * G + g] * 1125899906842624.0;
+      if (sc > 9.2e18) sc = 9.2e18;
+      if (sc < -9.2e18) sc = -9.2e18;
+      key[g] = (long long)sc / 4096 * 4096 + g;
+    }
+    for (int g = 0; g < G; ++g) {
+      int r = 0;
+      for (int h = 0; h < G; ++h) r += key[h] > key[g];
+      order[r] = g;
+    }
+    int* crep = rep + (size_t)s * G;
+    int* clen = size + (size_t)s * G;
+    for (int c = 0; c < G; ++c) { crep[c] = -1; clen[c] = 0; }
+    int ncl = 1;
+    crep[0] = order[0];
+    clen[0] = 1;
+    for (int i = 0; i < G; ++i) {
+      const int g = order[i];
+      const double* cur = bb + (size_t)g * nbb * 3;
+      int hit = -1;
+      for (int c = 0; c < ncl && hit < 0; ++c) {
+        const double* r = bb + (size_t)crep[c] * nbb * 3;
+        double sum = 0.0;
+        for (int a = 0; a < nbb; ++a) {
+          const double dx = r[a * 3] - cur[a * 3], dy = r[a * 3 + 1] - cur[a * 3 + 1], dz = r[a * 3 + 2] - cur[a * 3 + 2];
+          double t = 0.0;
+          t += dx * dx;
+          t += dy * dy;
+          t += dz * dz;
+          sum += t;
+        }
+        if (sqrt(sum / nbb) <= 4.0) hit = c;
+      }
+      if (hit < 0) { hit = ncl++; crep[hit] = g; }
+      ++clen[hit];
+      member[(size_t)s * G + g] = hit;
+    }
+    n_clusters[s] = ncl;
+  }
+  free(rec); free(lig); free(bb); free(key); free(order);
+}

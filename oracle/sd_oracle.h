@@ -87,6 +87,12 @@ void or_gso_step(const or_system* sys, or_state* st, const double* u_step /* [S]
 void or_init_state(const or_system* sys, or_state* st, const double* pos0,
                    double luciferin0, double vision0);
 
+/* Final-pose clustering of every swarm (BSAS of the reference's GPU pipeline variant,
+ * source/dock/src/cuda/pipeline:2766-2960, keys as prepare_pair, prepare_gso_task.cu:1170-1187):
+ * pos [S][G][pose_len], scores [S][G], backbone flags per receptor / ligand atom; outputs
+ * n_clusters [S], rep / size [S][G] (first n_clusters[s] used), member [S][G]. */
+void or_cluster(const or_system* sys, const double* pos, const double* scores, const int* rec_bb,
+                const int* lig_bb, int* n_clusters, int* rep, int* size, int* member);
 double or_sin_cr(double x);
 double or_acos_cr(double x);
 /* slerp of the reference (prepare_gso_tasks.cc:1370-1421) with cr or libm math */

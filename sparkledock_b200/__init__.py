@@ -214,6 +214,18 @@ class Docking:
         check(_abi.lib().sd_get_tuning(self._ctx, C.byref(v), C.byref(w), C.byref(mb), dptr(ms), n), "sd_get_tuning")
         return {"variant": v.value, "warps": w.value, "min_blocks": mb.value, "ms": [float(x) for x in ms]}
 
+    def cluster(self, ci: int, rec_backbone, lig_backbone) -> dict:
+        """BSAS clustering of the current poses of every swarm of complex ci (sd_cluster)."""
+        c = self._complexes[ci]
+        S, G = c.n_swarms, c.n_glowworms
+        rb = np.ascontiguousarray(rec_backbone, np.int32)
+        lb = np.ascontiguousarray(lig_backbone, np.int32)
+        ncl = np.empty(S, np.int32)
+        rep, size, member = (np.empty((S, G), np.int32) for _ in range(3))
+        check(_abi.lib().sd_cluster(self._ctx, ci, iptr(rb), iptr(lb), iptr(ncl), iptr(rep), iptr(size),
+                                    iptr(member)), "sd_cluster")
+        return {"n_clusters": ncl, "rep": rep, "size": size, "member": member}
+
     def set_precision(self, precision: int):
         check(_abi.lib().sd_set_precision(self._ctx, precision), "sd_set_precision")
 

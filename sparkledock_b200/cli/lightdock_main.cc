@@ -18,7 +18,8 @@
 //   "dfire_table": path of a DCparams-format file (168*168*20 values, one per line);
 //        absent: seeded synthetic table ("table_seed", default 3)
 // -s STEPS is honoured (the reference parses it but runs its compiled STEPS macro).
-// Output: <dir>/swarm_<i>/gso_<STEPS>.out as the reference GPU path writes them.
+// Output: <dir>/swarm_<i>/gso_<STEPS>.out as the reference GPU path writes them; with PDB inputs
+// also <dir>/swarm_<i>/cluster.repr (sd_cluster on the CA / P atoms).
 #include <errno.h>
 #include <sys/stat.h>
 #include <unistd.h>
@@ -323,6 +324,21 @@ int main(int argc, char** argv) {
   const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   sd_stats stats = {};
   if (!rc) rc = sd_get_stats(ctx, &stats);
+  // PDB inputs: cluster the final poses on their CA / P atoms (cluster.repr per swarm)
+  std::vector<int> ncl, crep, clen, cmem;
+  double cluster_secs = 0;
+  if (!rc && pdb_input) {
+    std::vector<int> rbb(desc.n_rec), lbb(desc.n_lig);
+    sd_structure_arrays(rec_s.get(), nullptr, nullptr, nullptr, rbb.data(), nullptr);
+    sd_structure_arrays(lig_s.get(), nullptr, nullptr, nullptr, lbb.data(), nullptr);
+    ncl.resize(swarms);
+    crep.resize(n);
+    clen.resize(n);
+    cmem.resize(n);
+    const auto c0 = std::chrono::steady_clock::now();
+    rc = sd_cluster(ctx, 0, rbb.data(), lbb.data(), ncl.data(), crep.data(), clen.data(), cmem.data());
+    cluster_secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - c0).count();
+  }
   if (rc) {
     const std::string m = sd_last_error();
     sd_ctx_destroy(ctx);
@@ -334,7 +350,11 @@ int main(int argc, char** argv) {
   if (sd_write_gso_output(outdir.c_str(), 0, swarms, G, pl, steps, pos.data(), luc.data(), nnei.data(), vis.data(),
                           sc.data()) != SD_OK)
     return die(sd_last_error());
+  if (pdb_input && sd_write_cluster_repr(outdir.c_str(), 0, swarms, G, ncl.data(), crep.data(), clen.data(),
+                                          sc.data()) != SD_OK)
+    return die(sd_last_error());
   printf("simulation execution:%f\n", secs);
+  if (pdb_input) printf("clustering: %f s (cluster.repr per swarm)\n", cluster_secs);
   printf("scored poses: %lld (%.0f per second, wall clock including setup and state transfers)\n",
          stats.scored_poses, stats.scored_poses / secs);
   return 0;

@@ -1185,4 +1185,70 @@ int sd_refine_poses(sd_ctx* c, int ci, double* poses, int n, int iters, double s
   return SD_OK;
 }
 
+int sd_cluster(sd_ctx* c, int ci, const int* rec_backbone, const int* lig_backbone, int* n_clusters,
+               int* cluster_rep, int* cluster_len, int* member_of) {
+  if (!c || ci < 0 || ci >= c->ncplx || !rec_backbone || !lig_backbone || !n_clusters || !cluster_rep ||
+      !cluster_len || !member_of)
+    return fail(SD_ERR_ARG, "sd_cluster: bad arguments");
+  if (!c->cx[ci].state_set) return fail(SD_ERR_STATE, "sd_cluster: no state");
+  const DevComplex& D = c->cx[ci].d;
+  const int S = D.S, G = D.G, nslots = D.ntiles * SD_TILE;
+  // receptor slot of each flagged atom (atoms are stored in spatial tile order)
+  std::vector<int> orig(nslots), slot_of(D.nr, -1), rb, lb;
+  SD_CUDA(cudaMemcpy(orig.data(), D.r_orig, sizeof(int) * nslots, cudaMemcpyDeviceToHost));
+  for (int sl = 0; sl < nslots; ++sl)
+    if (orig[sl] >= 0) slot_of[orig[sl]] = sl;
+  for (int i = 0; i < D.nr; ++i)
+    if (rec_backbone[i]) rb.push_back(slot_of[i]);
+  for (int j = 0; j < D.nl; ++j)
+    if (lig_backbone[j]) lb.push_back(j);
+  const int nbr = (int)rb.size(), nbl = (int)lb.size(), nbb = nbr + nbl;
+  if (nbb == 0) return fail(SD_ERR_ARG, "sd_cluster: no backbone atoms flagged");
+  if (cluster_smem_bytes(G, nbb) > 227 * 1024) return fail(SD_ERR_NOTSUP, "sd_cluster: too many backbone atoms");
+  // swarms per launch: coordinates of at most ~1 GiB on the device
+  const size_t per_swarm = (size_t)G * nbb * 3 * sizeof(double);
+  const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)S, ((size_t)1 << 30) / per_swarm));
+  int* d_rb = nullptr;
+  int* d_lb = nullptr;
+  int* d_out = nullptr;
+  double* d_bb = nullptr;
+  auto release = [&]() {
+    cudaFree(d_rb);
+    cudaFree(d_lb);
+    cudaFree(d_out);
+    cudaFree(d_bb);
+  };
+  auto cu = [&](cudaError_t e) {
+    if (e == cudaSuccess) return SD_OK;
+    release();
+    return fail(e == cudaErrorMemoryAllocation ? SD_ERR_OOM : SD_ERR_CUDA, std::string("sd_cluster: ") + cudaGetErrorString(e));
+  };
+  int rc;
+  if ((rc = cu(cudaMalloc(&d_rb, sizeof(int) * std::max(1, nbr))))) return rc;
+  if ((rc = cu(cudaMalloc(&d_lb, sizeof(int) * std::max(1, nbl))))) return rc;
+  if ((rc = cu(cudaMalloc(&d_out, sizeof(int) * ((size_t)S + 3 * (size_t)S * G))))) return rc;
+  if ((rc = cu(cudaMalloc(&d_bb, per_swarm * chunk)))) return rc;
+  if (nbr && (rc = cu(cudaMemcpy(d_rb, rb.data(), sizeof(int) * nbr, cudaMemcpyHostToDevice)))) return rc;
+  if (nbl && (rc = cu(cudaMemcpy(d_lb, lb.data(), sizeof(int) * nbl, cudaMemcpyHostToDevice)))) return rc;
+  int* d_ncl = d_out;
+  int* d_rep = d_out + S;
+  int* d_len = d_rep + (size_t)S * G;
+  int* d_mem = d_len + (size_t)S * G;
+  for (int s0 = 0; s0 < S; s0 += chunk) {
+    const int ns = std::min(chunk, S - s0);
+    if ((rc = cluster_launch(c->d_cplx, ci, s0, ns, G, d_rb, nbr, d_lb, nbl, d_bb, d_ncl, d_rep, d_len, d_mem,
+                             c->stream))) {
+      release();
+      return fail(rc, "sd_cluster: launch failed");
+    }
+  }
+  if ((rc = cu(cudaStreamSynchronize(c->stream)))) return rc;
+  if ((rc = cu(cudaMemcpy(n_clusters, d_ncl, sizeof(int) * S, cudaMemcpyDeviceToHost)))) return rc;
+  if ((rc = cu(cudaMemcpy(cluster_rep, d_rep, sizeof(int) * S * G, cudaMemcpyDeviceToHost)))) return rc;
+  if ((rc = cu(cudaMemcpy(cluster_len, d_len, sizeof(int) * S * G, cudaMemcpyDeviceToHost)))) return rc;
+  if ((rc = cu(cudaMemcpy(member_of, d_mem, sizeof(int) * S * G, cudaMemcpyDeviceToHost)))) return rc;
+  release();
+  return SD_OK;
+}
+
 }  // extern "C"

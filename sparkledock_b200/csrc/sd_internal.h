@@ -150,6 +150,10 @@ int pydock_launch(const ScoreLaunch& L, int precision, bool grad, double* out_gr
                   cudaStream_t st);
 int pydock_threads();
 void set_key_thresholds(const double* t64);
+size_t cluster_smem_bytes(int G, int nbb);
+int cluster_launch(const DevComplex* d_cplx, int ci, int s0, int ns, int G, const int* d_rb_slot, int nbr,
+                   const int* d_lb_idx, int nbl, double* d_bb, int* d_ncl, int* d_rep, int* d_len, int* d_member,
+                   cudaStream_t st);
 
 }  // namespace sd
 #endif  // __CUDACC__

@@ -70,6 +70,7 @@ def oracle():
         L.or_acos_cr.argtypes = [C.c_double]
         L.or_slerp.argtypes = [_dp, _dp, C.c_double, C.c_int]
         L.or_key_thresholds.argtypes = [_dp]
+        L.or_cluster.argtypes = [C.POINTER(OrSystem), _dp, _dp, _ip, _ip, _ip, _ip, _ip, _ip]
         L.or_pydock_energy.restype = C.c_double
         L.or_pydock_energy.argtypes = [C.POINTER(OrSystem), _dp]
         L.or_pydock_grad.argtypes = [C.POINTER(OrSystem), _dp, _dp]
@@ -215,3 +216,15 @@ def ref_structure(path: str, noxt: bool, noh: bool, now: bool, cap: int = 40000)
                                  _d(tr), cap)
     assert n >= 0
     return xyz[:n].copy(), mask[:n].copy(), dfire[:n].copy(), tr
+
+
+def oracle_cluster(osys: OracleSystem, pos, scores, rec_bb, lig_bb):
+    S, G = osys.S, osys.cx.n_glowworms
+    pos = np.ascontiguousarray(pos, np.float64)
+    scores = np.ascontiguousarray(scores, np.float64)
+    rb = np.ascontiguousarray(rec_bb, np.int32)
+    lb = np.ascontiguousarray(lig_bb, np.int32)
+    ncl = np.empty(S, np.int32)
+    rep, size, member = (np.empty((S, G), np.int32) for _ in range(3))
+    oracle().or_cluster(osys.ptr, _d(pos), _d(scores), _i(rb), _i(lb), _i(ncl), _i(rep), _i(size), _i(member))
+    return {"n_clusters": ncl, "rep": rep, "size": size, "member": member}

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import sparkledock_b200 as sd
-from oracle_bind import OracleState, OracleSystem, oracle_step
+from oracle_bind import OracleState, OracleSystem, oracle_cluster, oracle_step
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CLI = os.path.join(ROOT, "sparkledock_b200", "lightdock_b200")
@@ -122,3 +122,14 @@ def test_cli_pdb_inputs_match_oracle(tmp_path, tables):
     for sw in range(S):
         got = (tmp_path / f"swarm_{sw}" / f"gso_{steps}.out").read_text()
         assert got == exp[sw]
+    # cluster.repr from the oracle's clustering of the same final state on the CA atoms
+    cl = oracle_cluster(osys, st.pos, st.scoring, rs.backbone, ls.backbone)
+    for sw in range(S):
+        lines = [f"{c}:{cl['size'][sw, c]}:{fmt_g(st.scoring[sw, cl['rep'][sw, c]])}:{cl['rep'][sw, c]}:"
+                 f"lightdock_{cl['rep'][sw, c]}.pdb" for c in range(cl["n_clusters"][sw])]
+        assert (tmp_path / f"swarm_{sw}" / "cluster.repr").read_text() == "\n".join(lines) + "\n"
+
+
+def fmt_g(v):
+    """A double as an ostream prints it by default (6 significant digits, %g)."""
+    return "%g" % v

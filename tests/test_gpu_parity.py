@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import sparkledock_b200 as sd
-from oracle_bind import OracleState, OracleSystem, oracle_bins, oracle_scores, oracle_step
+from oracle_bind import OracleState, OracleSystem, oracle_bins, oracle_cluster, oracle_scores, oracle_step
 
 pytestmark = pytest.mark.gpu
 
@@ -274,3 +274,28 @@ def test_large_anm_extents_loose_tiles(variant, tables, monkeypatch):
         assert rel_err(en, ref_en).max() <= MIXED_TOL
         _, en64 = dk.score_poses(0, poses, sd.SD_PREC_FP64)
         assert np.array_equal(en64, ref_en)
+
+
+@pytest.mark.parametrize("precision", [sd.SD_PREC_FP64, sd.SD_PREC_MIXED])
+def test_cluster_final_poses_match_oracle(precision, tables):
+    """BSAS clustering of the final poses after GSO steps (sd_cluster) equals the oracle's on the
+    same state: cluster count, representatives, sizes and every glowworm's cluster."""
+    cx = sd.SyntheticComplex(757, 481, 3, 96, seed=71)
+    rb = (np.arange(cx.n_rec) % 8 == 1).astype(np.int32)  # a backbone-like subset
+    lb = (np.arange(cx.n_lig) % 8 == 1).astype(np.int32)
+    with sd.Docking([cx], tables, precision=precision) as dk:
+        dk.init_state(0, cx.poses)
+        dk.set_draws(0, sd.gso_draws(4, cx.n_swarms, 10, cx.n_glowworms))
+        dk.step(10)
+        st = dk.get_state(0)
+        got = dk.cluster(0, rb, lb)
+    ref = oracle_cluster(OracleSystem(cx, tables), st.pos, st.scoring, rb, lb)
+    assert np.array_equal(got["n_clusters"], ref["n_clusters"])
+    for s in range(cx.n_swarms):
+        n = ref["n_clusters"][s]
+        assert np.array_equal(got["rep"][s, :n], ref["rep"][s, :n])
+        assert np.array_equal(got["size"][s, :n], ref["size"][s, :n])
+    assert np.array_equal(got["member"], ref["member"])
+    # the first glowworm in score order is counted twice in cluster 0, as in the reference
+    assert (ref["size"].sum(axis=1) == cx.n_glowworms + 1).all()
+    assert 1 < ref["n_clusters"].min()
