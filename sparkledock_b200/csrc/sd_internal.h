@@ -67,12 +67,10 @@ struct DevComplex {
   const double* lc_xyz;    // [nlchunks*32][3]
   const double* lc_modes;  // [nml][nlchunks*32][3]
   const int* lc_mask;      // [nlchunks*32]
-  const int* lc_col;       // [nlchunks*32]
   const int* lc_colk;      // [nlchunks*32] key-indexed column base tL*32
   float lig_ctr[3];        // ligand centroid (ligand frame)
   float mnorm_r[SD_MAX_MODES], mnorm_l[SD_MAX_MODES];  // max per-atom mode norm (rounded up)
   float lig_radius;        // max |l0_j| (rounded up)
-  float rec_span;          // max |r0_i - origin| (rounded up)
   double lig_ref[3];
   // GSO state [S][G]
   double* pos;
@@ -99,7 +97,7 @@ struct StepCtl {
   unsigned long long stats[12];  // mirrors sd_stats order
 };
 
-enum { ST_SCORED = 0, ST_STEPS, ST_FALLBACK, ST_D2ZERO, ST_D2CUT, ST_UZERO, ST_SHORT, ST_TIMEOUT, ST_PAIRS, ST_EVALS, ST_GUARD };
+enum { ST_SCORED = 0, ST_STEPS, ST_FALLBACK, ST_D2ZERO, ST_D2CUT, ST_UZERO, ST_SHORT, ST_TIMEOUT, ST_PAIRS, ST_EVALS };
 
 struct GsoParamsDev {
   double rho, gamma, beta, max_vision, step_t, step_r, step_nm;
