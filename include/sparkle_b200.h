@@ -189,6 +189,17 @@ int sd_structure_arrays(const sd_structure* s, double* xyz, int* nm_mask, int* d
                         double* translation);
 int sd_structure_free(sd_structure* s);
 
+/* Normal modes of a structure (ANM), as the reference's setup computes them: cal_anm
+ * (source/dock/src/cal_anm.cc:61-219) with its GPU eigensolver (source/dock/src/cuda/cal_anm.cu:
+ * 28-91).  Coordinates re-centred on the mean of all atoms; CA atoms (else C4) as nodes; Hessian
+ * with cutoff 15 A, gamma 1 (built on `device`); the lowest n_modes + 6 eigenpairs from
+ * cuSOLVER syevd, those below 1e-6 dropped; every atom of residue i takes node i's components
+ * (one CA per residue required); modes normalised, then scaled to `rmsd` with the reference's
+ * draws over n_swarms x n_glowworms extents.  modes_out [n_modes][n_atoms][3] (the layout of
+ * sd_complex_desc.rec_modes / lig_modes); xyz_out [n_atoms][3], the re-centred coordinates the
+ * modes belong to (may be NULL); eigvals_out [n_modes] (may be NULL). */
+int sd_anm(const sd_structure* s, int n_modes, double rmsd, int n_swarms, int n_glowworms, int device,
+           double* modes_out, double* xyz_out, double* eigvals_out);
 /* Khachiyan minimum-volume enclosing ellipsoid centre of n points (tolerance 0.01), the ligand
  * reference point of minimum_volume_ellipsoid (source/dock/src/prepare_gso_tasks.cc:106-267). */
 int sd_reference_point(const double* xyz, int n, double* center);

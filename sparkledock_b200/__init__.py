@@ -98,6 +98,7 @@ class Structure:
     SD_PDB_NOXT | SD_PDB_NOH | SD_PDB_NOW (setup.json noxt / noh / now)."""
 
     def __init__(self, path: str, flags: int = 0):
+        self.path, self.flags = str(path), flags
         h = C.c_void_p()
         check(_abi.lib().sd_structure_load(str(path).encode(), flags, C.byref(h)), "sd_structure_load")
         try:
@@ -113,6 +114,22 @@ class Structure:
                                                  iptr(self.backbone), dptr(self.translation)), "sd_structure_arrays")
         finally:
             _abi.lib().sd_structure_free(h)
+
+    def anm(self, n_modes: int, rmsd: float, n_swarms: int, n_glowworms: int, device: int = 0):
+        """Normal modes as the reference's setup computes them (sd_anm): modes
+        [n_modes][n_atoms][3], the re-centred coordinates they belong to [n_atoms][3] and the
+        eigenvalues [n_modes]."""
+        h = C.c_void_p()
+        check(_abi.lib().sd_structure_load(self.path.encode(), self.flags, C.byref(h)), "sd_structure_load")
+        try:
+            modes = np.empty((n_modes, self.n_atoms, 3))
+            xyz = np.empty((self.n_atoms, 3))
+            lam = np.empty(n_modes)
+            check(_abi.lib().sd_anm(h, n_modes, rmsd, n_swarms, n_glowworms, device, dptr(modes), dptr(xyz),
+                                    dptr(lam)), "sd_anm")
+        finally:
+            _abi.lib().sd_structure_free(h)
+        return modes, xyz, lam
 
 
 def GsoParams(**kw) -> _abi.GsoParams:

@@ -10,9 +10,11 @@
 //   "precision": "mixed" | "fp64" | "fp64_ref"  (absent: mixed)
 //   "translation_step", "rotation_step", "nmodes_step"   (absent: the reference's 0.5)
 //   receptor_pdb, ligand_pdb, noxt, noh, now: the structures, read as the reference's setup
-//        reads them (sd_structure_load); ANM modes and pyDock charges are seeded stand-ins and
-//        the starting poses come from sd_starting_poses (ANM, charges and the reference's
-//        surface-based swarm placement are setup stages not built here)
+//        reads them (sd_structure_load); with use_anm, normal modes from sd_anm (cal_anm, which
+//        also re-centres each structure on its mean) with anm_rec_rmsd / anm_lig_rmsd (absent:
+//        0.5, lightdock's default); pyDock charges are seeded stand-ins and the starting poses
+//        come from sd_starting_poses (charges and the reference's surface-based swarm placement
+//        are setup stages not built here)
 //   "synthetic": {"receptor_atoms": N, "ligand_atoms": M, "seed": s}
 //        seeded synthetic receptor/ligand in place of receptor_pdb / ligand_pdb
 //   "dfire_table": path of a DCparams-format file (168*168*20 values, one per line);
@@ -269,16 +271,24 @@ int main(int argc, char** argv) {
   double* pos0 = nullptr;
   if (sd_synth_generate(&spec, buf.get(), &desc, &pos0) != SD_OK) return die(sd_last_error());
   if (pdb_input) {
-    // real coordinates, masks and DFIRE types; ANM modes and pyDock charges / LJ types stay the
-    // seeded stand-ins (ANM and charge assignment are setup stages not built here); reference
-    // point and starting poses from the real structures
+    // real coordinates, masks and DFIRE types; pyDock charges / LJ types stay the seeded
+    // stand-ins (charge assignment is a setup stage not built here); starting poses from the
+    // centred receptor (run_simulation places swarms before the ANM stage); ANM modes, which
+    // re-centre the structure as cal_anm does; the ligand reference point last, on the final
+    // coordinates (prepare_gso_tasks.cc:1201-1202)
     sd_structure_arrays(rec_s.get(), const_cast<double*>(desc.rec_xyz), const_cast<int*>(desc.rec_mask),
                         const_cast<int*>(desc.rec_dfire_type), nullptr, nullptr);
     sd_structure_arrays(lig_s.get(), const_cast<double*>(desc.lig_xyz), const_cast<int*>(desc.lig_mask),
                         const_cast<int*>(desc.lig_dfire_type), nullptr, nullptr);
-    if (sd_reference_point(desc.lig_xyz, desc.n_lig, desc.lig_ref_point) != SD_OK) return die(sd_last_error());
     if (sd_starting_poses(desc.rec_xyz, desc.n_rec, swarms, G, anm_rec, anm_lig, spec.seed, pos0) != SD_OK)
       return die(sd_last_error());
+    if (anm_rec > 0 && sd_anm(rec_s.get(), anm_rec, num_or(root, "anm_rec_rmsd", 0.5), swarms, G, device,
+                              const_cast<double*>(desc.rec_modes), const_cast<double*>(desc.rec_xyz), nullptr) != SD_OK)
+      return die(sd_last_error());
+    if (anm_lig > 0 && sd_anm(lig_s.get(), anm_lig, num_or(root, "anm_lig_rmsd", 0.5), swarms, G, device,
+                              const_cast<double*>(desc.lig_modes), const_cast<double*>(desc.lig_xyz), nullptr) != SD_OK)
+      return die(sd_last_error());
+    if (sd_reference_point(desc.lig_xyz, desc.n_lig, desc.lig_ref_point) != SD_OK) return die(sd_last_error());
   }
 
   const size_t tsz = (size_t)SD_DFIRE_TYPES * SD_DFIRE_TYPES * SD_DFIRE_BINS;

@@ -134,6 +134,17 @@ int dfire_type_of(int res, int atom) {
 
 }  // namespace
 
+namespace sd {
+// atoms of a loaded structure for the setup stages built on it (ANM)
+int structure_atoms(const sd_structure* s, std::vector<double>& xyz, std::vector<std::string>& names,
+                    std::vector<int>& residue_first) {
+  xyz = s->xyz;
+  names = s->atom_name;
+  residue_first = s->residue_first;
+  return SD_OK;
+}
+}  // namespace sd
+
 extern "C" {
 
 int sd_structure_load(const char* pdb_path, int flags, sd_structure** out) {

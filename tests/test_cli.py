@@ -86,8 +86,9 @@ def write_pdb(path, xyz, chain):
 @pytest.mark.gpu
 def test_cli_pdb_inputs_match_oracle(tmp_path, tables):
     """PDB inputs through the command line: structures read as the reference's setup reads them,
-    seeded ANM modes, reference point and starting poses from the real coordinates; the FP64 run's
-    output files equal the oracle's trajectory on the same complex."""
+    ANM modes from sd_anm (which re-centres each structure), starting poses and reference point
+    from the real coordinates; the FP64 run's output files equal the oracle's trajectory on the
+    same complex."""
     rec0 = sd.SyntheticComplex(400, 248, 1, 4, seed=31)
     write_pdb(tmp_path / "rec.pdb", rec0.rec_xyz + 20.0, "A")
     write_pdb(tmp_path / "lig.pdb", rec0.lig_xyz - 7.0, "B")
@@ -108,11 +109,13 @@ def test_cli_pdb_inputs_match_oracle(tmp_path, tables):
     cx.lig_xyz[:] = ls.xyz
     cx.lig_mask[:] = ls.nm_mask
     cx.lig_type[:] = ls.dfire_type
+    poses = np.empty_like(cx.poses)
+    sd._abi.lib().sd_starting_poses(sd.dptr(cx.rec_xyz), rs.n_atoms, S, G, 10, 10, seed, sd.dptr(poses))
+    cx.rec_modes[:], cx.rec_xyz[:], _ = rs.anm(10, 0.5, S, G)
+    cx.lig_modes[:], cx.lig_xyz[:], _ = ls.anm(10, 0.5, S, G)
     ref = np.empty(3)
     sd._abi.lib().sd_reference_point(sd.dptr(cx.lig_xyz), ls.n_atoms, sd.dptr(ref))
     cx.lig_ref = ref
-    poses = np.empty_like(cx.poses)
-    sd._abi.lib().sd_starting_poses(sd.dptr(cx.rec_xyz), rs.n_atoms, S, G, 10, 10, seed, sd.dptr(poses))
     osys = OracleSystem(cx, tables)
     st = OracleState(S, G, cx.pose_len, poses)
     U = sd.gso_draws(0, S, steps, G)
