@@ -204,13 +204,30 @@ int sd_anm(const sd_structure* s, int n_modes, double rmsd, int n_swarms, int n_
  * reference point of minimum_volume_ellipsoid (source/dock/src/prepare_gso_tasks.cc:106-267). */
 int sd_reference_point(const double* xyz, int n, double* center);
 /* Seeded starting poses [n_swarms][n_glowworms][pose_len] around a receptor centred at the
- * origin: swarm centres at uniform directions on a shell 10 A outside its bounding sphere, each
- * glowworm at its centre plus N(0, 2 A) per axis, a uniform random unit quaternion and N(0, 1)
- * ANM extents.  A stand-in for the reference's surface-based swarm placement
- * (calculate_start_pos, source/prep/src/initialization.cc), which is a setup stage not built
- * here. */
+ * origin, for synthetic complexes (no residues to place swarms on): swarm centres at uniform
+ * directions on a shell 10 A outside its bounding sphere, each glowworm at its centre plus
+ * N(0, 2 A) per axis, a uniform random unit quaternion and N(0, 1) ANM extents.  Structures read
+ * from PDB files are placed by sd_place_swarms. */
 int sd_starting_poses(const double* rec_xyz, int n_rec, int n_swarms, int n_glowworms, int n_modes_rec,
                       int n_modes_lig, unsigned long long seed, double* poses);
+
+/* Swarm centres and starting poses as the reference's setup places them: calculate_start_pos
+ * (source/dock/src/cal_anm.cc:775-990) with calculate_surface_point (:541-774) and the k-means
+ * of source/dock/src/kmeans.cc:126-241, on the structures as read (before centring).  Surface
+ * atoms clustered into n_swarms centroids (k-means++ from mt19937(324324), 100 Lloyd
+ * iterations); 100 sphere points around each at the surface distance (10 A, or a quarter of the
+ * ligand's diameter when that is >= 20 A), those near another centroid or within 3 A of the
+ * receptor dropped; the rest clustered into the swarm centres (500 iterations), moved into the
+ * centred frame.  Poses: per swarm and glowworm a point in the swarm_radius ball (lightdock's
+ * default 10), a uniform quaternion (mt19937(starting_points_seed + rank) doubles) and, with
+ * use_anm, N(0, 1) extents from std::default_random_engine(anm_seed), receptor modes first
+ * (without use_anm the extents are 0).  The k-means and filters run on `device`, bit-identical
+ * to the reference.  centers_out [n_swarms][3] (may be NULL); poses_out
+ * [n_swarms][n_glowworms][7 + n_modes_rec + n_modes_lig] (may be NULL).  Fails where the
+ * reference is undefined: no more surface atoms or kept points than swarms, or an empty cluster. */
+int sd_place_swarms(const sd_structure* receptor, const sd_structure* ligand, int n_swarms, int n_glowworms,
+                    int n_modes_rec, int n_modes_lig, int use_anm, int starting_points_seed, int anm_seed,
+                    double swarm_radius, int rank, int device, double* centers_out, double* poses_out);
 
 /* Final-pose clustering of every swarm of complex ci (BSAS, as the reference's GPU pipeline
  * variant clusters before writing cluster.repr, source/dock/src/cuda/pipeline:2766-2960):

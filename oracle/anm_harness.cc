@@ -18,6 +18,7 @@
 #include "initialization.h"
 #include "mpi.h"
 #include "read_input_structure.h"
+#include "swarm_centers.h"
 #include "translate.h"
 
 int MPI_Abort(MPI_Comm, int code) {
@@ -49,6 +50,33 @@ int ref_cal_anm(const char* path, int noxt, int noh, int now, int n_modes, doubl
   if (n > cap) return -1;
   std::memcpy(modes, c.modes, sizeof(double) * (size_t)c.n_modes * n * 3);
   std::memcpy(xyz, c.atom_coordinates, sizeof(double) * (size_t)n * 3);
+  return n;
+}
+
+// The reference's swarm placement (calculate_start_pos, source/dock/src/cal_anm.cc:775-990) on
+// two structures set up as run_simulation does before it (read, centring translation computed but
+// not applied): swarm centres [swarms][3] and poses [swarms][glowworms][7 + anm_rec + anm_lig].
+// swarms > 0 (the SASA-derived count is not driven), no membrane, no dense sampling.
+int ref_start_positions(const char* rec_path, const char* lig_path, int noxt, int noh, int now, int swarms,
+                        int glowworms, int seed, int anm_seed, int anm_rec, int anm_lig, int use_anm,
+                        double swarm_radius, double* centers, double* poses) {
+  Complex rec, lig;
+  read_input_structure(rec, rec_path, noxt != 0, noh != 0, now != 0, false, (int)strlen(rec_path));
+  read_input_structure(lig, lig_path, noxt != 0, noh != 0, now != 0, false, (int)strlen(lig_path));
+  init_center_translate(rec.translation, rec.atom_coordinates, rec.elements, rec.structure_size, rec.num_atoms,
+                        rec.num_structures);
+  init_center_translate(lig.translation, lig.atom_coordinates, lig.elements, lig.structure_size, lig.num_atoms,
+                        lig.num_structures);
+  SwarmCenters c;
+  calculate_start_pos(c, rec, lig, swarms, glowworms, seed, rec.translation, lig.translation, 50.0, use_anm != 0,
+                      anm_seed, anm_rec, anm_lig, false, false, false, swarm_radius, false, 0.0, 0, false, rec_path, 0,
+                      1);
+  std::memcpy(centers, c.s, sizeof(double) * 3 * c.swarms);
+  const int pl = 7 + anm_rec + anm_lig;
+  for (size_t i = 0; i < (size_t)c.swarms * glowworms; ++i)
+    for (int k = 0; k < pl; ++k) poses[i * pl + k] = (k < 7 || use_anm) ? c.pos[i * pl + k] : 0.0;
+  const int n = c.swarms;
+  free_swarmcenters(c);
   return n;
 }
 

@@ -132,6 +132,28 @@ class Structure:
         return modes, xyz, lam
 
 
+def place_swarms(receptor: Structure, ligand: Structure, n_swarms: int, n_glowworms: int, n_modes_rec: int = 0,
+                 n_modes_lig: int = 0, use_anm: bool = True, starting_points_seed: int = 324324,
+                 anm_seed: int = 324324, swarm_radius: float = 10.0, rank: int = 0, device: int = 0):
+    """Swarm centres [n_swarms][3] (centred receptor frame) and starting poses
+    [n_swarms][n_glowworms][7 + modes] as the reference's setup places them (sd_place_swarms)."""
+    lib = _abi.lib()
+    hr, hl = C.c_void_p(), C.c_void_p()
+    check(lib.sd_structure_load(receptor.path.encode(), receptor.flags, C.byref(hr)), "sd_structure_load")
+    try:
+        check(lib.sd_structure_load(ligand.path.encode(), ligand.flags, C.byref(hl)), "sd_structure_load")
+        centers = np.empty((n_swarms, 3))
+        poses = np.empty((n_swarms, n_glowworms, 7 + n_modes_rec + n_modes_lig))
+        check(lib.sd_place_swarms(hr, hl, n_swarms, n_glowworms, n_modes_rec, n_modes_lig, int(use_anm),
+                                  starting_points_seed, anm_seed, swarm_radius, rank, device, dptr(centers),
+                                  dptr(poses)), "sd_place_swarms")
+    finally:
+        lib.sd_structure_free(hr)
+        if hl.value:
+            lib.sd_structure_free(hl)
+    return centers, poses
+
+
 def GsoParams(**kw) -> _abi.GsoParams:
     p = _abi.GsoParams()
     _abi.lib().sd_gso_params_default(C.byref(p))

@@ -95,6 +95,8 @@ SIGNATURES = {
     "sd_structure_load": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]),
     "sd_reference_point": (C.c_int, [_dp, C.c_int, _dp]),
     "sd_anm": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp]),
+    "sd_place_swarms": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                  C.c_int, C.c_double, C.c_int, C.c_int, _dp, _dp]),
     "sd_cluster": (C.c_int, [C.c_void_p, C.c_int, _ip, _ip, _ip, _ip, _ip, _ip]),
     "sd_write_cluster_repr": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, _ip, _ip, _ip, _dp]),
     "sd_starting_poses": (C.c_int, [_dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_ulonglong, _dp]),

@@ -12,9 +12,10 @@
 //   receptor_pdb, ligand_pdb, noxt, noh, now: the structures, read as the reference's setup
 //        reads them (sd_structure_load); with use_anm, normal modes from sd_anm (cal_anm, which
 //        also re-centres each structure on its mean) with anm_rec_rmsd / anm_lig_rmsd (absent:
-//        0.5, lightdock's default); pyDock charges are seeded stand-ins and the starting poses
-//        come from sd_starting_poses (charges and the reference's surface-based swarm placement
-//        are setup stages not built here)
+//        0.5, lightdock's default); swarm centres and starting poses from sd_place_swarms (the
+//        reference's surface-based placement) with starting_points_seed, anm_seed (absent:
+//        324324) and swarm_radius (absent: 10); membrane, transmembrane and dense_sampling are
+//        refused (the reference leaves them undeveloped); pyDock charges are seeded stand-ins
 //   "synthetic": {"receptor_atoms": N, "ligand_atoms": M, "seed": s}
 //        seeded synthetic receptor/ligand in place of receptor_pdb / ligand_pdb
 //   "dfire_table": path of a DCparams-format file (168*168*20 values, one per line);
@@ -272,16 +273,24 @@ int main(int argc, char** argv) {
   if (sd_synth_generate(&spec, buf.get(), &desc, &pos0) != SD_OK) return die(sd_last_error());
   if (pdb_input) {
     // real coordinates, masks and DFIRE types; pyDock charges / LJ types stay the seeded
-    // stand-ins (charge assignment is a setup stage not built here); starting poses from the
-    // centred receptor (run_simulation places swarms before the ANM stage); ANM modes, which
-    // re-centre the structure as cal_anm does; the ligand reference point last, on the final
-    // coordinates (prepare_gso_tasks.cc:1201-1202)
+    // stand-ins (charge assignment is a setup stage not built here); swarm placement and
+    // starting poses as run_simulation.cc:66-74 places them (before the ANM stage, on the
+    // structures as read); ANM modes, which re-centre the structure as cal_anm does; the ligand
+    // reference point last, on the final coordinates (prepare_gso_tasks.cc:1201-1202)
     sd_structure_arrays(rec_s.get(), const_cast<double*>(desc.rec_xyz), const_cast<int*>(desc.rec_mask),
                         const_cast<int*>(desc.rec_dfire_type), nullptr, nullptr);
     sd_structure_arrays(lig_s.get(), const_cast<double*>(desc.lig_xyz), const_cast<int*>(desc.lig_mask),
                         const_cast<int*>(desc.lig_dfire_type), nullptr, nullptr);
-    if (sd_starting_poses(desc.rec_xyz, desc.n_rec, swarms, G, anm_rec, anm_lig, spec.seed, pos0) != SD_OK)
+    for (const char* k : {"membrane", "transmembrane", "dense_sampling"}) {
+      const JVal* v = root.get(k);
+      if (v && v->kind == JVal::Bool && v->b) return die(std::string("setup.json: \"") + k + "\" is not supported");
+    }
+    const auto p0 = std::chrono::steady_clock::now();
+    if (sd_place_swarms(rec_s.get(), lig_s.get(), swarms, G, anm_rec, anm_lig, use_anm ? 1 : 0,
+                        (int)num_or(root, "starting_points_seed", 324324), (int)num_or(root, "anm_seed", 324324),
+                        num_or(root, "swarm_radius", 10.0), 0, device, nullptr, pos0) != SD_OK)
       return die(sd_last_error());
+    const auto p1 = std::chrono::steady_clock::now();
     if (anm_rec > 0 && sd_anm(rec_s.get(), anm_rec, num_or(root, "anm_rec_rmsd", 0.5), swarms, G, device,
                               const_cast<double*>(desc.rec_modes), const_cast<double*>(desc.rec_xyz), nullptr) != SD_OK)
       return die(sd_last_error());
@@ -289,6 +298,9 @@ int main(int argc, char** argv) {
                               const_cast<double*>(desc.lig_modes), const_cast<double*>(desc.lig_xyz), nullptr) != SD_OK)
       return die(sd_last_error());
     if (sd_reference_point(desc.lig_xyz, desc.n_lig, desc.lig_ref_point) != SD_OK) return die(sd_last_error());
+    const auto p2 = std::chrono::steady_clock::now();
+    printf("setup: swarm placement %f s, ANM %f s\n", std::chrono::duration<double>(p1 - p0).count(),
+           std::chrono::duration<double>(p2 - p1).count());
   }
 
   const size_t tsz = (size_t)SD_DFIRE_TYPES * SD_DFIRE_TYPES * SD_DFIRE_BINS;

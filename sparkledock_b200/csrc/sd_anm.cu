@@ -71,12 +71,6 @@ __global__ void hessian_diag_kernel(const double* xyz, int n, double cutoff2, do
 }  // namespace
 }  // namespace sd
 
-struct sd_structure;
-namespace sd {
-// accessors of sd_structure (sd_structure.cc)
-int structure_atoms(const sd_structure* s, std::vector<double>& xyz, std::vector<std::string>& names,
-                    std::vector<int>& residue_first);
-}  // namespace sd
 
 extern "C" int sd_anm(const sd_structure* s, int n_modes, double rmsd, int n_swarms, int n_glowworms, int device,
                       double* modes_out, double* xyz_out, double* eigvals_out) {

@@ -3,6 +3,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "../../include/sparkle_b200.h"
 
@@ -31,6 +32,14 @@ namespace sd {
 // thread-local error message; returns code
 int fail(int code, const std::string& msg);
 void mvee_center(const double* p, int n, double tol, double* center);
+
+// accessors of sd_structure (sd_structure.cc)
+int structure_atoms(const sd_structure* s, std::vector<double>& xyz, std::vector<std::string>& names,
+                    std::vector<int>& residue_first);
+const std::vector<double>& structure_raw_xyz(const sd_structure* s);
+const std::vector<std::string>& structure_residue_names(const sd_structure* s);
+const std::vector<int>& structure_residue_first(const sd_structure* s);
+const double* structure_translation(const sd_structure* s);
 
 }  // namespace sd
 

@@ -27,6 +27,7 @@
 
 struct sd_structure {
   std::vector<double> xyz;          // translated (centred) coordinates [n][3]
+  std::vector<double> raw_xyz;      // coordinates as read (through float), before centring
   std::vector<int> mask, dfire, backbone;
   std::vector<std::string> atom_name, residue_name, element;
   std::vector<int> residue_first;   // [n_res + 1] first atom of each residue
@@ -143,6 +144,11 @@ int structure_atoms(const sd_structure* s, std::vector<double>& xyz, std::vector
   residue_first = s->residue_first;
   return SD_OK;
 }
+
+const std::vector<double>& structure_raw_xyz(const sd_structure* s) { return s->raw_xyz; }
+const std::vector<std::string>& structure_residue_names(const sd_structure* s) { return s->residue_name; }
+const std::vector<int>& structure_residue_first(const sd_structure* s) { return s->residue_first; }
+const double* structure_translation(const sd_structure* s) { return s->translation; }
 }  // namespace sd
 
 extern "C" {
@@ -221,6 +227,7 @@ int sd_structure_load(const char* pdb_path, int flags, sd_structure** out) {
       tz += s->xyz[i * 3 + 2];
       ++dim;
     }
+  s->raw_xyz = s->xyz;
   s->translation[0] = -1 * tx / dim;
   s->translation[1] = -1 * ty / dim;
   s->translation[2] = -1 * tz / dim;

@@ -10,6 +10,7 @@ import pytest
 
 import sparkledock_b200 as sd
 from oracle_bind import OracleState, OracleSystem, oracle_cluster, oracle_step
+from test_anm import protein_pdb
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CLI = os.path.join(ROOT, "sparkledock_b200", "lightdock_b200")
@@ -73,25 +74,14 @@ def test_cli_fp64_run_matches_oracle(tmp_path, tables):
         assert got == exp[s]
 
 
-def write_pdb(path, xyz, chain):
-    """A PDB of glycines (N, CA, C, O per residue) at the given coordinates (4 atoms per residue)."""
-    names = ("N", "CA", "C", "O")
-    with open(path, "w") as f:
-        for i, (x, y, z) in enumerate(xyz):
-            f.write("ATOM  %5d  %-3s GLY %s%4d    %8.3f%8.3f%8.3f  1.00  0.00\n" % (i + 1, names[i % 4], chain,
-                                                                              i // 4 + 1, x, y, z))
-        f.write("END\n")
-
-
 @pytest.mark.gpu
 def test_cli_pdb_inputs_match_oracle(tmp_path, tables):
     """PDB inputs through the command line: structures read as the reference's setup reads them,
-    ANM modes from sd_anm (which re-centres each structure), starting poses and reference point
-    from the real coordinates; the FP64 run's output files equal the oracle's trajectory on the
-    same complex."""
-    rec0 = sd.SyntheticComplex(400, 248, 1, 4, seed=31)
-    write_pdb(tmp_path / "rec.pdb", rec0.rec_xyz + 20.0, "A")
-    write_pdb(tmp_path / "lig.pdb", rec0.lig_xyz - 7.0, "B")
+    swarms placed by sd_place_swarms, ANM modes from sd_anm (which re-centres each structure),
+    reference point from the final coordinates; the FP64 run's output files equal the oracle's
+    trajectory on the same complex."""
+    protein_pdb(tmp_path / "rec.pdb", 110, 31)
+    protein_pdb(tmp_path / "lig.pdb", 45, 32)
     seed, S, G, steps = 19, 2, 40, 6
     setup = {"swarms": S, "glowworms": G, "anm_rec": 10, "anm_lig": 10, "use_anm": True, "precision": "fp64",
              "scoring": "dfire", "receptor_pdb": "rec.pdb", "ligand_pdb": "lig.pdb", "noxt": True, "noh": True,
@@ -109,8 +99,7 @@ def test_cli_pdb_inputs_match_oracle(tmp_path, tables):
     cx.lig_xyz[:] = ls.xyz
     cx.lig_mask[:] = ls.nm_mask
     cx.lig_type[:] = ls.dfire_type
-    poses = np.empty_like(cx.poses)
-    sd._abi.lib().sd_starting_poses(sd.dptr(cx.rec_xyz), rs.n_atoms, S, G, 10, 10, seed, sd.dptr(poses))
+    _, poses = sd.place_swarms(rs, ls, S, G, 10, 10, True, seed, 324324)
     cx.rec_modes[:], cx.rec_xyz[:], _ = rs.anm(10, 0.5, S, G)
     cx.lig_modes[:], cx.lig_xyz[:], _ = ls.anm(10, 0.5, S, G)
     ref = np.empty(3)
