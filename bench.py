@@ -16,9 +16,11 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import shutil
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -270,6 +272,77 @@ def run_e2e(cfg, steps, device, seed=0):
     return {"ms": ms, "wall_s": wall, "scored": scored, "h2d": h2d, "d2h": d2h}
 
 
+SETUP_FILES = ("setup_receptor.pdb", "setup_ligand.pdb")
+
+
+def setup_structures(cfg, folder):
+    """Synthetic compact chains (glycines and alanines, 4.33 atoms per residue) of about the
+    first complex's atom counts, written to folder; returns their paths."""
+    import sparkledock_b200 as sd
+    nr, nl, _ = cfg["complexes"][0]
+    paths = [os.path.join(folder, f) for f in SETUP_FILES]
+    sd.synthetic_protein_pdb(paths[0], int(round(nr * 3 / 13)), 7)
+    sd.synthetic_protein_pdb(paths[1], int(round(nl * 3 / 13)), 8)
+    return paths
+
+
+def time_setup(cfg, folder, device):
+    """Wall clock of the setup stages that prepare a docking run from PDB files, on synthetic
+    chains of the first complex's size: swarm placement (sd_place_swarms: the receptor-surface
+    k-means, sphere filters and starting poses of every swarm x glowworm) and the ANM modes of
+    both structures (sd_anm).  Each after one untimed call."""
+    import sparkledock_b200 as sd
+    rp, lp = setup_structures(cfg, folder)
+    flags = sd.SD_PDB_NOXT | sd.SD_PDB_NOH | sd.SD_PDB_NOW
+    rec, lig = sd.Structure(rp, flags), sd.Structure(lp, flags)
+    S = cfg["complexes"][0][2]
+    out = {"receptor_atoms": rec.n_atoms, "ligand_atoms": lig.n_atoms, "swarms": S, "glowworms": G}
+    sd.place_swarms(rec, lig, S, G, 10, 10, True, 324324, 324324, device=device)
+    t0 = time.perf_counter()
+    sd.place_swarms(rec, lig, S, G, 10, 10, True, 324324, 324324, device=device)
+    out["placement_ms"] = (time.perf_counter() - t0) * 1e3
+    for st, key in ((rec, "anm_receptor_ms"), (lig, "anm_ligand_ms")):
+        st.anm(10, 0.5, S, G, device)
+        t0 = time.perf_counter()
+        st.anm(10, 0.5, S, G, device)
+        out[key] = (time.perf_counter() - t0) * 1e3
+    return out
+
+
+def cpu_reference_placement(cfg, folder, device):
+    """The reference's own swarm placement (calculate_start_pos, compiled unmodified into
+    oracle/_ref/libsdref_anm.so) on the same synthetic chains, wall clock on the host, and whether
+    its centres and poses equal sd_place_swarms'."""
+    import ctypes as C
+    import sparkledock_b200 as sd
+    so = os.path.join(ROOT, "oracle", "_ref", "libsdref_anm.so")
+    if not os.path.exists(so):
+        return {"value": None, "error": "reference harness not built"}
+    rp, lp = [os.path.join(folder, f) for f in SETUP_FILES]
+    S = cfg["complexes"][0][2]
+    dp = C.POINTER(C.c_double)
+    L = C.CDLL(so)
+    L.ref_start_positions.argtypes = [C.c_char_p, C.c_char_p] + [C.c_int] * 10 + [C.c_double, dp, dp]
+    cent = np.zeros((S, 3))
+    poses = np.zeros((S, G, 27))
+    sys.stdout.flush()
+    saved = os.dup(1)
+    os.dup2(2, 1)  # the reference reports its progress on stdout; keep stdout for the JSON line
+    try:
+        t0 = time.perf_counter()
+        L.ref_start_positions(rp.encode(), lp.encode(), 1, 1, 1, S, G, 324324, 324324, 10, 10, 1, 10.0,
+                              cent.ctypes.data_as(dp), poses.ctypes.data_as(dp))
+        dt = time.perf_counter() - t0
+    finally:
+        os.dup2(saved, 1)
+        os.close(saved)
+    flags = sd.SD_PDB_NOXT | sd.SD_PDB_NOH | sd.SD_PDB_NOW
+    c2, p2 = sd.place_swarms(sd.Structure(rp, flags), sd.Structure(lp, flags), S, G, 10, 10, True, 324324, 324324,
+                             device=device)
+    return {"placement_ms": dt * 1e3, "cores": 1, "kind": "reference",
+            "bit_identical": bool(np.array_equal(cent, c2) and np.array_equal(poses, p2))}
+
+
 def cpu_reference_rate(cfg, budget_s=12.0, seed=0):
     """The reference's own CPU scoring path (oracle/_ref: its compiled cdfire_calculate_dfire,
     rotate and GSO helpers, OpenMP over swarms) on a bounded swarm sample; falls back to the
@@ -401,6 +474,8 @@ def main():
     spot = fp64_spot_check(run["ctx"], run["cxs"]) if cfg["precision"] == "mixed" else None
     clustering = time_clustering(run["ctx"], run["cxs"])
     run["ctx"].close()
+    setup_dir = tempfile.mkdtemp(prefix="sd_setup_") if rank == 0 else None
+    setup = time_setup(cfg, setup_dir, device) if rank == 0 else None
 
     extra = {}
     if not args.no_fp64 and cfg["precision"] == "mixed":
@@ -450,6 +525,7 @@ def main():
         "autotuner": tuning,
         "fp64_spot_check": spot,
         "final_clustering": clustering,
+        "setup": setup,
         **({"per_step": {"scored_poses": run["per_step"], "ms": run["ms"]}} if args.per_step else {}),
         "edge_counts": {k: stats[k] for k in ("pairs_fallback", "edge_d2_zero", "edge_d2_cutoff", "edge_u_zero",
                                               "edge_shortfall")},
@@ -488,6 +564,11 @@ def main():
                                     if k in ("value", "unit", "cores", "kind", "sample")}
         except Exception as e:  # the baseline is reported, never required
             line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+        try:
+            setup["reference_cpu"] = cpu_reference_placement(cfg, setup_dir, device)
+        except Exception as e:
+            setup["reference_cpu"] = {"value": None, "error": str(e)[:200]}
+    shutil.rmtree(setup_dir, ignore_errors=True)
     print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()

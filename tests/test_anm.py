@@ -26,42 +26,7 @@ FLAGS = sd.SD_PDB_NOXT | sd.SD_PDB_NOH | sd.SD_PDB_NOW
 _dp = C.POINTER(C.c_double)
 
 
-def protein_pdb(path, n_res, seed):
-    """A compact synthetic chain of glycines and alanines (N, CA, C, O [, CB]): CA steps of 3.8 A
-    inside a sphere, no two CA closer than 3.4 A.  Returns (atom names, first atom of each residue)."""
-    rng = np.random.default_rng(seed)
-    radius = 2.6 * n_res ** (1.0 / 3.0) + 6.0
-    ca = [np.zeros(3)]
-    while len(ca) < n_res:
-        step = rng.normal(size=3)
-        p = ca[-1] + step * (3.8 / np.linalg.norm(step))
-        if np.linalg.norm(p) > radius or np.min(np.linalg.norm(np.array(ca) - p, axis=1)) < 3.4:
-            if rng.random() < 0.02:  # back out of a dead end
-                ca.pop() if len(ca) > 1 else None
-            continue
-        ca.append(p)
-
-    def bond(origin, length):
-        v = rng.normal(size=3)
-        return origin + v * (length / np.linalg.norm(v))
-
-    names, first, lines = [], [], []
-    for r, p in enumerate(ca):
-        first.append(len(names))
-        res = "ALA" if r % 3 == 1 else "GLY"
-        c = bond(p, 1.52)
-        atoms = [("N", bond(p, 1.46)), ("CA", p), ("C", c), ("O", bond(c, 1.23))]
-        if res == "ALA":
-            atoms.append(("CB", bond(p, 1.53)))
-        for nm, x in atoms:
-            names.append(nm)
-            lines.append("ATOM  %5d  %-3s %s A%4d    %8.3f%8.3f%8.3f  1.00  0.00\n" %
-                         (len(names), nm, res, r + 1, x[0] + 30.0, x[1] - 12.0, x[2] + 5.0))
-    first.append(len(names))
-    with open(path, "w") as f:
-        f.writelines(lines)
-        f.write("END\n")
-    return names, first
+protein_pdb = sd.synthetic_protein_pdb
 
 
 def _anm_lib():
