@@ -189,6 +189,18 @@ int sd_structure_arrays(const sd_structure* s, double* xyz, int* nm_mask, int* d
                         double* translation);
 int sd_structure_free(sd_structure* s);
 
+/* One pose written as the reference writes its lightdock_<g>.pdb files (write_pdb,
+ * source/dock/src/prepare_gso_tasks.cc:1279-1345; the pipeline variant's final writer,
+ * source/dock/src/cuda/pipeline:2599-2750): the receptor's atoms then the ligand's, each numbered
+ * from 1, every record with the fields as read (record name, atom name, alternate location,
+ * residue name and number, chain, insertion code, occupancy, B-factor, element) and the given
+ * coordinates [n_atoms][3] (e.g. from sd_materialise_poses), %.3f / %.2f in the PDB columns.
+ * ligand and lig_xyz may both be NULL.  Fails where the reference's column padding would be
+ * negative (it throws there): more than 99,999 atoms, a residue name over 3 characters, a residue
+ * number over 4, or a coordinate that needs more than 8 columns. */
+int sd_write_pose_pdb(const char* path, const sd_structure* receptor, const double* rec_xyz,
+                      const sd_structure* ligand, const double* lig_xyz);
+
 /* Normal modes of a structure (ANM), as the reference's setup computes them: cal_anm
  * (source/dock/src/cal_anm.cc:61-219) with its GPU eigensolver (source/dock/src/cuda/cal_anm.cu:
  * 28-91).  Coordinates re-centred on the mean of all atoms; CA atoms (else C4) as nodes; Hessian
@@ -228,6 +240,15 @@ int sd_starting_poses(const double* rec_xyz, int n_rec, int n_swarms, int n_glow
 int sd_place_swarms(const sd_structure* receptor, const sd_structure* ligand, int n_swarms, int n_glowworms,
                     int n_modes_rec, int n_modes_lig, int use_anm, int starting_points_seed, int anm_seed,
                     double swarm_radius, int rank, int device, double* centers_out, double* poses_out);
+
+/* Every atom of chosen glowworms of complex complex_idx at their current (final) poses, through
+ * the exact FP64 transforms the scorer uses (receptor ANM; ligand ANM, rotation, translation), as
+ * the reference materialises the final poses for its lightdock_<g>.pdb files (prepare_receptor /
+ * prepare_ligand after the last step, source/dock/src/cuda/pipeline:2492-2500).  poses[k] =
+ * swarm * n_glowworms + glowworm; rec_xyz_out [n][n_rec][3] and lig_xyz_out [n][n_lig][3] in the
+ * atom order of sd_complex_desc (either may be NULL). */
+int sd_materialise_poses(sd_ctx* ctx, int complex_idx, const int* poses, int n, double* rec_xyz_out,
+                         double* lig_xyz_out);
 
 /* Final-pose clustering of every swarm of complex ci (BSAS, as the reference's GPU pipeline
  * variant clusters before writing cluster.repr, source/dock/src/cuda/pipeline:2766-2960):

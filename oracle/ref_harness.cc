@@ -17,8 +17,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
 #include <random>
 #include <string>
+#include <vector>
 
 #include "complex.h"
 #include "fastdfire.h"
@@ -314,6 +316,23 @@ int ref_load_structure(const char* path, int noxt, int noh, int now, double* xyz
   memcpy(translation, c.translation, sizeof(double) * 3);
   delete[] objs;
   return n;
+}
+
+// The reference's pose file writer (write_pdb, prepare_gso_tasks.cc:1279-1345, the format of the
+// pipeline's lightdock_<g>.pdb files) for a receptor and a ligand read by read_input_structure,
+// with the given coordinates [n][3] of each, into out_path (receptor atoms, then ligand atoms).
+// Returns 0, or -1 when the file cannot be opened.
+int ref_write_pose_pdb(const char* rec_path, const char* lig_path, int noxt, int noh, int now,
+                       const double* rec_xyz, const double* lig_xyz, const char* out_path) {
+  Complex r, l;
+  read_input_structure(r, rec_path, noxt != 0, noh != 0, now != 0, false, (int)strlen(rec_path));
+  read_input_structure(l, lig_path, noxt != 0, noh != 0, now != 0, false, (int)strlen(lig_path));
+  std::ofstream f(out_path);
+  if (!f.is_open()) return -1;
+  std::vector<double> rc(rec_xyz, rec_xyz + (size_t)3 * r.num_atoms), lc(lig_xyz, lig_xyz + (size_t)3 * l.num_atoms);
+  write_pdb(r, f, rc.data());
+  write_pdb(l, f, lc.data());
+  return 0;
 }
 
 }  // extern "C"

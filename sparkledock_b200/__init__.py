@@ -16,7 +16,7 @@ from . import _abi
 from ._abi import (SD_PDB_NOH, SD_PDB_NOW, SD_PDB_NOXT, SD_PREC_FP64, SD_PREC_FP64_REF,  # noqa: F401
                    SD_PREC_MIXED, SD_SCORING_DFIRE, SD_SCORING_PYDOCK, SparkleError, check, dptr, iptr)
 
-__all__ = ["SyntheticComplex", "Structure", "synthetic_tables", "synthetic_protein_pdb", "place_swarms", "gso_draws", "mixed_variant_count", "GsoParams", "Docking",
+__all__ = ["SyntheticComplex", "Structure", "synthetic_tables", "synthetic_protein_pdb", "place_swarms", "write_pose_pdb", "gso_draws", "mixed_variant_count", "GsoParams", "Docking",
            "SD_PREC_FP64_REF", "SD_PREC_FP64", "SD_PREC_MIXED", "SD_SCORING_DFIRE",
            "SD_SCORING_PYDOCK", "SparkleError", "device_count"]
 
@@ -130,6 +130,28 @@ class Structure:
         finally:
             _abi.lib().sd_structure_free(h)
         return modes, xyz, lam
+
+
+def write_pose_pdb(path, receptor: Structure, rec_xyz, ligand: Structure = None, lig_xyz=None) -> None:
+    """Write one pose as the reference writes lightdock_<g>.pdb (sd_write_pose_pdb): the
+    receptor's atoms at rec_xyz [n_rec][3], then the ligand's at lig_xyz."""
+    lib = _abi.lib()
+    hr, hl = C.c_void_p(), C.c_void_p()
+    check(lib.sd_structure_load(receptor.path.encode(), receptor.flags, C.byref(hr)), "sd_structure_load")
+    try:
+        rx = np.ascontiguousarray(rec_xyz, np.float64)
+        lx = None
+        if ligand is not None:
+            check(lib.sd_structure_load(ligand.path.encode(), ligand.flags, C.byref(hl)), "sd_structure_load")
+            lx = np.ascontiguousarray(lig_xyz, np.float64)
+        if rx.shape != (receptor.n_atoms, 3) or (lx is not None and lx.shape != (ligand.n_atoms, 3)):
+            raise ValueError("coordinates must be [n_atoms][3] for each structure")
+        check(lib.sd_write_pose_pdb(str(path).encode(), hr, dptr(rx), hl if ligand is not None else None,
+                                    dptr(lx) if lx is not None else None), "sd_write_pose_pdb")
+    finally:
+        lib.sd_structure_free(hr)
+        if hl.value:
+            lib.sd_structure_free(hl)
 
 
 def place_swarms(receptor: Structure, ligand: Structure, n_swarms: int, n_glowworms: int, n_modes_rec: int = 0,
@@ -264,6 +286,17 @@ class Docking:
         check(_abi.lib().sd_cluster(self._ctx, ci, iptr(rb), iptr(lb), iptr(ncl), iptr(rep), iptr(size),
                                     iptr(member)), "sd_cluster")
         return {"n_clusters": ncl, "rep": rep, "size": size, "member": member}
+
+    def materialise(self, ci: int, poses):
+        """Every atom of the chosen glowworms (index swarm * n_glowworms + glowworm) of complex ci at
+        their current poses (sd_materialise_poses): receptor [n][n_rec][3], ligand [n][n_lig][3]."""
+        c = self._complexes[ci]
+        idx = np.ascontiguousarray(poses, np.int32).ravel()
+        rec = np.empty((idx.size, c.n_rec, 3))
+        lig = np.empty((idx.size, c.n_lig, 3))
+        check(_abi.lib().sd_materialise_poses(self._ctx, ci, iptr(idx), idx.size, dptr(rec), dptr(lig)),
+              "sd_materialise_poses")
+        return rec, lig
 
     def set_precision(self, precision: int):
         check(_abi.lib().sd_set_precision(self._ctx, precision), "sd_set_precision")

@@ -22,11 +22,16 @@
 //        absent: seeded synthetic table ("table_seed", default 3)
 // -s STEPS is honoured (the reference parses it but runs its compiled STEPS macro).
 // Output: <dir>/swarm_<i>/gso_<STEPS>.out as the reference GPU path writes them; with PDB inputs
-// also <dir>/swarm_<i>/cluster.repr (sd_cluster on the CA / P atoms).
+// also <dir>/swarm_<i>/cluster.repr (sd_cluster on the CA / P atoms) and the final poses as
+// <dir>/swarm_<i>/lightdock_<g>.pdb (sd_materialise_poses + sd_write_pose_pdb, the reference
+// pipeline's format), per "write_poses": "representatives" (absent: the glowworms cluster.repr
+// names), "all" (every glowworm, as the reference's pipeline writes them) or "none".
 #include <errno.h>
 #include <sys/stat.h>
 #include <unistd.h>
 
+#include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -34,8 +39,10 @@
 #include <fstream>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/sparkle_b200.h"
@@ -225,6 +232,7 @@ int main(int argc, char** argv) {
   if (scoring < 0) return die("setup.json: \"scoring\" must be \"dfire\" or \"pydock\"");
   int precision = prec_s == "mixed" ? SD_PREC_MIXED : prec_s == "fp64" ? SD_PREC_FP64 : prec_s == "fp64_ref" ? SD_PREC_FP64_REF : -1;
   if (precision < 0) return die("setup.json: \"precision\" must be \"mixed\", \"fp64\" or \"fp64_ref\"");
+  std::string write_poses = "none";
   const JVal* syn = root.get("synthetic");
   const bool pdb_input = !syn || syn->kind != JVal::Obj;
   // PDB inputs: structures read as the reference's setup reads them (flags noxt / noh / now)
@@ -281,6 +289,9 @@ int main(int argc, char** argv) {
                         const_cast<int*>(desc.rec_dfire_type), nullptr, nullptr);
     sd_structure_arrays(lig_s.get(), const_cast<double*>(desc.lig_xyz), const_cast<int*>(desc.lig_mask),
                         const_cast<int*>(desc.lig_dfire_type), nullptr, nullptr);
+    write_poses = str_or(root, "write_poses", "representatives");
+    if (write_poses != "representatives" && write_poses != "all" && write_poses != "none")
+      return die("setup.json: \"write_poses\" must be \"representatives\", \"all\" or \"none\"");
     for (const char* k : {"membrane", "transmembrane", "dense_sampling"}) {
       const JVal* v = root.get(k);
       if (v && v->kind == JVal::Bool && v->b) return die(std::string("setup.json: \"") + k + "\" is not supported");
@@ -361,22 +372,71 @@ int main(int argc, char** argv) {
     rc = sd_cluster(ctx, 0, rbb.data(), lbb.data(), ncl.data(), crep.data(), clen.data(), cmem.data());
     cluster_secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - c0).count();
   }
-  if (rc) {
-    const std::string m = sd_last_error();
+  auto fail_ctx = [&](const std::string& m) {
     sd_ctx_destroy(ctx);
     return die(m);
-  }
-  sd_ctx_destroy(ctx);
+  };
+  if (rc) return fail_ctx(sd_last_error());
   if (!outdir.empty() && outdir != "." && mkdir(outdir.c_str(), 0755) != 0 && errno != EEXIST)
-    return die("cannot create output directory " + outdir);
+    return fail_ctx("cannot create output directory " + outdir);
   if (sd_write_gso_output(outdir.c_str(), 0, swarms, G, pl, steps, pos.data(), luc.data(), nnei.data(), vis.data(),
                           sc.data()) != SD_OK)
-    return die(sd_last_error());
+    return fail_ctx(sd_last_error());
   if (pdb_input && sd_write_cluster_repr(outdir.c_str(), 0, swarms, G, ncl.data(), crep.data(), clen.data(),
                                           sc.data()) != SD_OK)
-    return die(sd_last_error());
+    return fail_ctx(sd_last_error());
+  // PDB inputs: final poses as swarm_<s>/lightdock_<g>.pdb, for the cluster representatives (the
+  // files cluster.repr names), every glowworm (as the reference's pipeline writes them), or none
+  double pose_secs = 0;
+  long long pose_files = 0;
+  if (pdb_input && write_poses != "none") {
+    const auto w0 = std::chrono::steady_clock::now();
+    std::vector<int> which;
+    for (int sw = 0; sw < swarms; ++sw) {
+      if (write_poses == "all") {
+        for (int g = 0; g < G; ++g) which.push_back(sw * G + g);
+      } else {
+        for (int c = 0; c < ncl[sw]; ++c) which.push_back(sw * G + crep[(size_t)sw * G + c]);
+      }
+    }
+    const size_t per_pose = (size_t)(desc.n_rec + desc.n_lig) * 3;
+    const int batch = (int)std::max<size_t>(1, std::min<size_t>(which.size(), ((size_t)256 << 20) / (per_pose * 8)));
+    std::vector<double> rx((size_t)batch * desc.n_rec * 3), lx((size_t)batch * desc.n_lig * 3);
+    const std::string base = outdir.empty() ? "." : outdir;
+    for (size_t k0 = 0; k0 < which.size(); k0 += batch) {
+      const int m = (int)std::min<size_t>(batch, which.size() - k0);
+      if (sd_materialise_poses(ctx, 0, which.data() + k0, m, rx.data(), lx.data()) != SD_OK)
+        return fail_ctx(sd_last_error());
+      // the files are independent: format and write them on every host core
+      std::atomic<int> next{0}, failed{0};
+      std::string first_error;
+      std::mutex err_mu;
+      auto worker = [&]() {
+        for (int k = next++; k < m && !failed; k = next++) {
+          const int sw = which[k0 + k] / G, g = which[k0 + k] % G;
+          const std::string path =
+              base + "/swarm_" + std::to_string(sw) + "/lightdock_" + std::to_string(g) + ".pdb";
+          if (sd_write_pose_pdb(path.c_str(), rec_s.get(), rx.data() + (size_t)k * desc.n_rec * 3, lig_s.get(),
+                                lx.data() + (size_t)k * desc.n_lig * 3) != SD_OK) {
+            std::lock_guard<std::mutex> lk(err_mu);
+            if (!failed++) first_error = sd_last_error();
+          }
+        }
+      };
+      const int nthreads = (int)std::max(1u, std::min(std::thread::hardware_concurrency(), 64u));
+      std::vector<std::thread> pool;
+      for (int t = 1; t < nthreads; ++t) pool.emplace_back(worker);
+      worker();
+      for (auto& th : pool) th.join();
+      if (failed) return fail_ctx(first_error);
+      pose_files += m;
+    }
+    pose_secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
+  }
+  sd_ctx_destroy(ctx);
   printf("simulation execution:%f\n", secs);
   if (pdb_input) printf("clustering: %f s (cluster.repr per swarm)\n", cluster_secs);
+  if (pose_files) printf("pose files: %lld lightdock_<g>.pdb in %f s\n", pose_files, pose_secs);
   printf("scored poses: %lld (%.0f per second, wall clock including setup and state transfers)\n",
          stats.scored_poses, stats.scored_poses / secs);
   return 0;

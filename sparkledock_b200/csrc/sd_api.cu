@@ -1178,6 +1178,62 @@ int sd_refine_poses(sd_ctx* c, int ci, double* poses, int n, int iters, double s
   return SD_OK;
 }
 
+int sd_materialise_poses(sd_ctx* c, int ci, const int* poses, int n, double* rec_xyz_out, double* lig_xyz_out) {
+  if (!c || ci < 0 || ci >= c->ncplx || !poses || n <= 0 || (!rec_xyz_out && !lig_xyz_out))
+    return fail(SD_ERR_ARG, "sd_materialise_poses: bad arguments");
+  if (!c->cx[ci].state_set) return fail(SD_ERR_STATE, "sd_materialise_poses: no state");
+  const DevComplex& D = c->cx[ci].d;
+  const long long SG = (long long)D.S * D.G;
+  for (int k = 0; k < n; ++k)
+    if (poses[k] < 0 || poses[k] >= SG) return fail(SD_ERR_ARG, "sd_materialise_poses: pose index out of range");
+  const int nr = D.nr, nl = D.nl, nslots = D.ntiles * SD_TILE;
+  std::vector<int> orig(nslots), slot_of(nr, 0);
+  SD_CUDA(cudaMemcpy(orig.data(), D.r_orig, sizeof(int) * nslots, cudaMemcpyDeviceToHost));
+  for (int sl = 0; sl < nslots; ++sl)
+    if (orig[sl] >= 0) slot_of[orig[sl]] = sl;
+  // poses per launch: coordinates of at most 256 MiB on the device
+  const size_t per_pose = (size_t)(nr + nl) * 3 * sizeof(double);
+  const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)n, ((size_t)256 << 20) / per_pose));
+  int *d_poses = nullptr, *d_slot = nullptr;
+  double* d_xyz = nullptr;
+  auto release = [&]() {
+    cudaFree(d_poses);
+    cudaFree(d_slot);
+    cudaFree(d_xyz);
+  };
+  auto cu = [&](cudaError_t e) {
+    if (e == cudaSuccess) return SD_OK;
+    release();
+    return fail(e == cudaErrorMemoryAllocation ? SD_ERR_OOM : SD_ERR_CUDA,
+                std::string("sd_materialise_poses: ") + cudaGetErrorString(e));
+  };
+  int rc;
+  if ((rc = cu(cudaMalloc(&d_poses, sizeof(int) * chunk)))) return rc;
+  if ((rc = cu(cudaMalloc(&d_slot, sizeof(int) * std::max(1, nr))))) return rc;
+  if ((rc = cu(cudaMalloc(&d_xyz, per_pose * chunk)))) return rc;
+  if ((rc = cu(cudaMemcpy(d_slot, slot_of.data(), sizeof(int) * nr, cudaMemcpyHostToDevice)))) return rc;
+  for (int k0 = 0; k0 < n; k0 += chunk) {
+    const int m = std::min(chunk, n - k0);
+    double* d_rec = d_xyz;
+    double* d_lig = d_xyz + (size_t)m * nr * 3;
+    if ((rc = cu(cudaMemcpyAsync(d_poses, poses + k0, sizeof(int) * m, cudaMemcpyHostToDevice, c->stream))))
+      return rc;
+    if ((rc = materialise_launch(c->d_cplx, ci, d_poses, m, d_slot, nr, nl, d_rec, d_lig, c->stream))) {
+      release();
+      return fail(rc, "sd_materialise_poses: launch failed");
+    }
+    if (rec_xyz_out && (rc = cu(cudaMemcpyAsync(rec_xyz_out + (size_t)k0 * nr * 3, d_rec, sizeof(double) * m * nr * 3,
+                                                cudaMemcpyDeviceToHost, c->stream))))
+      return rc;
+    if (lig_xyz_out && (rc = cu(cudaMemcpyAsync(lig_xyz_out + (size_t)k0 * nl * 3, d_lig, sizeof(double) * m * nl * 3,
+                                                cudaMemcpyDeviceToHost, c->stream))))
+      return rc;
+    if ((rc = cu(cudaStreamSynchronize(c->stream)))) return rc;
+  }
+  release();
+  return SD_OK;
+}
+
 int sd_cluster(sd_ctx* c, int ci, const int* rec_backbone, const int* lig_backbone, int* n_clusters,
                int* cluster_rep, int* cluster_len, int* member_of) {
   if (!c || ci < 0 || ci >= c->ncplx || !rec_backbone || !lig_backbone || !n_clusters || !cluster_rep ||

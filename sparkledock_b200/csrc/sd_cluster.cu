@@ -129,7 +129,40 @@ __global__ void __launch_bounds__(kClusterThreads) bsas_kernel(const DevComplex*
   if (tid == 0) n_clusters[s] = ncl;
 }
 
+// every atom of chosen glowworms (pose index swarm * G + glowworm): rec [n][nr][3] in the
+// caller's atom order (rslot maps it to the tile slots), lig [n][nl][3]
+__global__ void materialise_poses_kernel(const DevComplex* cplx, int ci, const int* poses, int n, const int* rslot,
+                                         int nr, int nl, double* rec, double* lig) {
+  const DevComplex& C = cplx[ci];
+  const int na = nr + nl, nslots = nslots_of(C);
+  const long long total = (long long)n * na;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(i / na), a = (int)(i % na);
+    const double* pose = C.pos + (size_t)poses[k] * C.pl;
+    double x, y, z, *o;
+    if (a < nr) {
+      receptor_exact(C, nslots, rslot[a], pose, x, y, z);
+      o = rec + ((size_t)k * nr + a) * 3;
+    } else {
+      double q[4] = {pose[3], pose[4], pose[5], pose[6]}, qi[4];
+      quat_inverse(q, qi);
+      ligand_exact(C, a - nr, pose, q, qi, x, y, z);
+      o = lig + ((size_t)k * nl + (a - nr)) * 3;
+    }
+    o[0] = x;
+    o[1] = y;
+    o[2] = z;
+  }
+}
+
 }  // namespace
+
+int materialise_launch(const DevComplex* d_cplx, int ci, const int* d_poses, int n, const int* d_rslot, int nr, int nl,
+                       double* d_rec, double* d_lig, cudaStream_t st) {
+  materialise_poses_kernel<<<148 * 8, 256, 0, st>>>(d_cplx, ci, d_poses, n, d_rslot, nr, nl, d_rec, d_lig);
+  return cudaGetLastError() == cudaSuccess ? SD_OK : SD_ERR_CUDA;
+}
 
 size_t cluster_smem_bytes(int G, int nbb) {
   return (size_t)G * 8 + (size_t)G * 4 * 3 + ((G & 1) ? 4 : 0) + (size_t)nbb * 24;

@@ -158,6 +158,8 @@ int pydock_launch(const ScoreLaunch& L, int precision, bool grad, double* out_gr
 int pydock_threads();
 void set_key_thresholds(const double* t64);
 size_t cluster_smem_bytes(int G, int nbb);
+int materialise_launch(const DevComplex* d_cplx, int ci, const int* d_poses, int n, const int* d_rslot, int nr, int nl,
+                       double* d_rec, double* d_lig, cudaStream_t st);
 int cluster_launch(const DevComplex* d_cplx, int ci, int s0, int ns, int G, const int* d_rb_slot, int nbr,
                    const int* d_lb_idx, int nbl, double* d_bb, int* d_ncl, int* d_rep, int* d_len, int* d_member,
                    cudaStream_t st);

@@ -16,6 +16,7 @@
 // membrane bead (MMB BJ) is an error (the reference's typing skips it without advancing, which
 // shifts every later atom's type).
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
@@ -31,6 +32,10 @@ struct sd_structure {
   std::vector<int> mask, dfire, backbone;
   std::vector<std::string> atom_name, residue_name, element;
   std::vector<int> residue_first;   // [n_res + 1] first atom of each residue
+  // the remaining fields of each atom's record, as read_atom_line keeps them for write_pdb
+  std::vector<std::string> record, alt, resname, chain, icode;  // columns 1-6 (untrimmed), 17, 18-21, 22, 27
+  std::vector<int> resnum;                             // columns 23-26
+  std::vector<float> occupancy, bfactor;               // columns 55-60, 61-66
   double translation[3] = {0, 0, 0};
 };
 
@@ -46,6 +51,19 @@ std::string trim(const std::string& s) {
 std::string field(const std::string& line, size_t pos, size_t len) {
   if (pos >= line.size()) return std::string();
   return line.substr(pos, len);
+}
+
+// occupancy / B-factor as read_atom_line reads them: std::stof of the 6-character field, the
+// default when the field is absent, unparsable or not consumed to its end
+float numeric_field(const std::string& line, size_t pos, float dflt) {
+  try {
+    const std::string f = line.substr(pos, 6);
+    size_t used = 0;
+    const float v = std::stof(f, &used);
+    return used < f.size() ? dflt : v;
+  } catch (...) {
+    return dflt;
+  }
 }
 
 const char* const kElements[12] = {"C", "N", "O", "H", "S", "P", "CL", "MG", "FE", "PB", "SE", "F"};
@@ -200,6 +218,14 @@ int sd_structure_load(const char* pdb_path, int flags, sd_structure** out) {
       s->xyz.push_back((double)(float)std::strtod(field(line, 30 + 8 * k, 8).c_str(), nullptr));
     s->atom_name.push_back(name);
     s->element.push_back(trim(elem));
+    s->record.push_back(line.substr(0, 6));
+    s->alt.push_back(trim(field(line, 16, 1)));
+    s->resname.push_back(res);
+    s->chain.push_back(trim(field(line, 21, 1)));
+    s->icode.push_back(ins);
+    s->resnum.push_back(res_num);
+    s->occupancy.push_back(numeric_field(line, 54, 1.0f));
+    s->bfactor.push_back(numeric_field(line, 60, 0.0f));
     if (first_residue || res != last_res_name || res_num != last_res_num || ins != last_ins) {
       first_residue = false;
       last_res_name = res;
@@ -278,6 +304,54 @@ int sd_structure_arrays(const sd_structure* s, double* xyz, int* nm_mask, int* d
 
 int sd_structure_free(sd_structure* s) {
   delete s;
+  return SD_OK;
+}
+
+int sd_write_pose_pdb(const char* path, const sd_structure* receptor, const double* rec_xyz,
+                      const sd_structure* ligand, const double* lig_xyz) {
+  if (!path || !receptor || !rec_xyz || (!ligand) != (!lig_xyz))
+    return sd::fail(SD_ERR_ARG, "sd_write_pose_pdb: bad arguments");
+  // left-pad (or right-pad) a field to width w; false where the reference's padding would be
+  // negative (it throws there)
+  auto pad = [](const std::string& v, size_t w, bool left, std::string& out) {
+    if (v.size() > w) return false;
+    out += left ? std::string(w - v.size(), ' ') + v : v + std::string(w - v.size(), ' ');
+    return true;
+  };
+  auto fixed = [](double v, int prec) {
+    char b[64];
+    std::snprintf(b, sizeof b, "%.*f", prec, v);
+    return std::string(b);
+  };
+  std::string text;
+  for (int part = 0; part < 2; ++part) {
+    const sd_structure* st = part == 0 ? receptor : ligand;
+    const double* xyz = part == 0 ? rec_xyz : lig_xyz;
+    if (!st) continue;
+    for (size_t i = 0; i < st->atom_name.size(); ++i) {
+      std::string ln = st->record[i];
+      std::string name = st->atom_name[i];
+      if (name.size() < 4) name = " " + name;
+      bool ok = pad(std::to_string(i + 1), 5, true, ln);
+      ln += " ";
+      ok = ok && pad(name, 4, false, ln) && pad(st->alt[i], 1, false, ln) &&
+           pad(st->resname[i], 3, true, ln) && pad(st->chain[i], 2, true, ln) &&
+           pad(std::to_string(st->resnum[i]), 4, true, ln) && pad(st->icode[i], 1, true, ln);
+      ln += "   ";
+      for (int k = 0; k < 3 && ok; ++k) ok = pad(fixed(xyz[i * 3 + k], 3), 8, true, ln);
+      ok = ok && pad(fixed(st->occupancy[i], 2), 6, true, ln) && pad(fixed(st->bfactor[i], 2), 6, true, ln) &&
+           pad(st->element[i], 12, true, ln);
+      if (!ok)
+        return sd::fail(SD_ERR_ARG, "sd_write_pose_pdb: atom " + std::to_string(i + 1) +
+                                        " does not fit the PDB columns (serial, residue or coordinate too wide)");
+      text += ln;
+      text += "\n";
+    }
+  }
+  FILE* f = std::fopen(path, "w");
+  if (!f) return sd::fail(SD_ERR_ARG, std::string("sd_write_pose_pdb: cannot open ") + path);
+  const bool good = std::fwrite(text.data(), 1, text.size(), f) == text.size();
+  if (std::fclose(f) != 0 || !good) return sd::fail(SD_ERR_ARG, std::string("sd_write_pose_pdb: cannot write ") + path);
   return SD_OK;
 }
 

@@ -95,6 +95,8 @@ def ref():
         L.ref_min_volume_ellipsoid.argtypes = [_dp, C.c_int, _dp, _dp]
         L.ref_load_structure.restype = C.c_int
         L.ref_load_structure.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, _dp, _ip, _ip, _dp, C.c_int]
+        L.ref_write_pose_pdb.restype = C.c_int
+        L.ref_write_pose_pdb.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.c_int, _dp, _dp, C.c_char_p]
         L.ref_run_cal_gso_tasks_cpu.restype = C.c_int
         L.ref_run_cal_gso_tasks_cpu.argtypes = [C.POINTER(OrSystem), _dp, C.c_int, C.c_char_p, C.c_int]
         _ref = L
@@ -216,6 +218,17 @@ def ref_structure(path: str, noxt: bool, noh: bool, now: bool, cap: int = 40000)
                                  _d(tr), cap)
     assert n >= 0
     return xyz[:n].copy(), mask[:n].copy(), dfire[:n].copy(), tr
+
+
+def oracle_pose_atoms(osys: OracleSystem, pose):
+    """Every receptor and ligand atom at one pose (the oracle's exact FP64 transforms)."""
+    pose = np.ascontiguousarray(pose, np.float64)
+    rec = np.empty((osys.cx.n_rec, 3))
+    lig = np.empty((osys.cx.n_lig, 3))
+    refp = np.empty(3)
+    oracle().or_receptor_pose(osys.ptr, _d(pose), _d(rec))
+    oracle().or_ligand_pose(osys.ptr, _d(pose), _d(lig), _d(refp))
+    return rec, lig
 
 
 def oracle_cluster(osys: OracleSystem, pos, scores, rec_bb, lig_bb):

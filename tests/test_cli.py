@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import sparkledock_b200 as sd
-from oracle_bind import OracleState, OracleSystem, oracle_cluster, oracle_step
+from oracle_bind import OracleState, OracleSystem, oracle_cluster, oracle_pose_atoms, oracle_step
 from test_anm import protein_pdb
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -120,6 +120,16 @@ def test_cli_pdb_inputs_match_oracle(tmp_path, tables):
         lines = [f"{c}:{cl['size'][sw, c]}:{fmt_g(st.scoring[sw, cl['rep'][sw, c]])}:{cl['rep'][sw, c]}:"
                  f"lightdock_{cl['rep'][sw, c]}.pdb" for c in range(cl["n_clusters"][sw])]
         assert (tmp_path / f"swarm_{sw}" / "cluster.repr").read_text() == "\n".join(lines) + "\n"
+    # one lightdock_<g>.pdb per representative, the oracle's final atoms in the reference's format
+    for sw in range(S):
+        reps = {int(cl["rep"][sw, c]) for c in range(cl["n_clusters"][sw])}
+        files = {int(f.name[len("lightdock_"):-4]) for f in (tmp_path / f"swarm_{sw}").glob("lightdock_*.pdb")}
+        assert files == reps
+        for g in reps:
+            r, l = oracle_pose_atoms(osys, st.pos[sw, g])
+            sd.write_pose_pdb(tmp_path / "expected.pdb", rs, r, ls, l)
+            assert (tmp_path / f"swarm_{sw}" / f"lightdock_{g}.pdb").read_bytes() == \
+                (tmp_path / "expected.pdb").read_bytes()
 
 
 def fmt_g(v):
