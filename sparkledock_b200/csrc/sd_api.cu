@@ -1182,6 +1182,7 @@ int sd_materialise_poses(sd_ctx* c, int ci, const int* poses, int n, double* rec
   if (!c || ci < 0 || ci >= c->ncplx || !poses || n <= 0 || (!rec_xyz_out && !lig_xyz_out))
     return fail(SD_ERR_ARG, "sd_materialise_poses: bad arguments");
   if (!c->cx[ci].state_set) return fail(SD_ERR_STATE, "sd_materialise_poses: no state");
+  SD_CUDA(cudaSetDevice(c->device));
   const DevComplex& D = c->cx[ci].d;
   const long long SG = (long long)D.S * D.G;
   for (int k = 0; k < n; ++k)
@@ -1240,6 +1241,7 @@ int sd_cluster(sd_ctx* c, int ci, const int* rec_backbone, const int* lig_backbo
       !cluster_len || !member_of)
     return fail(SD_ERR_ARG, "sd_cluster: bad arguments");
   if (!c->cx[ci].state_set) return fail(SD_ERR_STATE, "sd_cluster: no state");
+  SD_CUDA(cudaSetDevice(c->device));
   const DevComplex& D = c->cx[ci].d;
   const int S = D.S, G = D.G, nslots = D.ntiles * SD_TILE;
   // receptor slot of each flagged atom (atoms are stored in spatial tile order)

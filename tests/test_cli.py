@@ -39,6 +39,15 @@ def test_cli_usage_and_setup_errors(tmp_path):
     sc.write_text(json.dumps({"swarms": 2, "scoring": "vina", "synthetic": {"receptor_atoms": 50, "ligand_atoms": 40}}))
     r = run(["-f", str(sc)])
     assert r.returncode != 0 and "scoring" in r.stderr
+    # PDB inputs: option values checked before any device work
+    protein_pdb(tmp_path / "r.pdb", 30, 1)
+    protein_pdb(tmp_path / "l.pdb", 10, 2)
+    for extra, word in (({"write_poses": "some"}, "write_poses"), ({"membrane": True}, "membrane"),
+                        ({"dense_sampling": True}, "dense_sampling")):
+        f = tmp_path / "opt.json"
+        f.write_text(json.dumps({"swarms": 2, "receptor_pdb": "r.pdb", "ligand_pdb": "l.pdb", **extra}))
+        r = run(["-f", str(f)], cwd=tmp_path)
+        assert r.returncode != 0 and word in r.stderr, r.stderr
 
 
 def gso_lines(st, pl):
