@@ -87,11 +87,17 @@ __global__ void max_pair_d2_kernel(const double* xyz, int n, unsigned long long*
 }
 
 // k-means++ seeding (kmeans_init_centers3), one CTA.  prob[k-1] is round k's uniform draw.
+// kShared: the nearest-distance array lives in shared memory (n <= kSeedSmemPoints), else in
+// mind_global.  The two chains of a round stay strictly sequential; their loads are issued in
+// blocks of kChainBlock ahead of the dependent adds.
+constexpr int kChainBlock = 16;
+
+template <bool kShared>
 __global__ void __launch_bounds__(kSeedThreads) kpp_seed_kernel(const double* pts, int n, int K, int first,
                                                                   const double* prob, double* mind_global,
                                                                   double* centers) {
   extern __shared__ double mind_shared[];
-  double* mind = n <= kSeedSmemPoints ? mind_shared : mind_global;
+  double* mind = kShared ? mind_shared : mind_global;
   __shared__ int sel;
   const int tid = threadIdx.x;
   for (int k = tid; k < K; k += blockDim.x)
@@ -106,15 +112,33 @@ __global__ void __launch_bounds__(kSeedThreads) kpp_seed_kernel(const double* pt
     }
     __syncthreads();
     if (tid == 0) {
+      // the sum of the distances, in point order
       double sum = 0.0;
-      for (int p = 0; p < n; ++p) sum = __dadd_rn(sum, mind[p]);
+      int p = 0;
+      for (; p + kChainBlock <= n; p += kChainBlock) {
+        double v[kChainBlock];
+#pragma unroll
+        for (int j = 0; j < kChainBlock; ++j) v[j] = mind[p + j];
+#pragma unroll
+        for (int j = 0; j < kChainBlock; ++j) sum = __dadd_rn(sum, v[j]);
+      }
+      for (; p < n; ++p) sum = __dadd_rn(sum, mind[p]);
       sum = __dmul_rn(sum, prob[k - 1]);
+      // the running subtraction: the first point at which it is no longer positive
       int s = -1;
-      for (int p = 0; p < n; ++p) {
+      for (p = 0; p + kChainBlock <= n && s < 0; p += kChainBlock) {
+        double v[kChainBlock];
+#pragma unroll
+        for (int j = 0; j < kChainBlock; ++j) v[j] = mind[p + j];
+#pragma unroll
+        for (int j = 0; j < kChainBlock; ++j) {
+          sum = __dsub_rn(sum, v[j]);
+          if (s < 0 && !(sum > 0)) s = p + j;
+        }
+      }
+      for (; p < n && s < 0; ++p) {
         sum = __dsub_rn(sum, mind[p]);
-        if (sum > 0) continue;
-        s = p;
-        break;
+        if (!(sum > 0)) s = p;
       }
       sel = s;
     }
@@ -256,10 +280,14 @@ int kmeans(const double* d_pts, int n, int K, int iters, std::vector<double>& ce
       (e = cudaMemset(d_group, 0xff, sizeof(int) * n)) || (e = cudaMemset(d_changed, 0, sizeof(int) * iters)) ||
       (e = cudaMemset(d_done, 0, sizeof(int))))
     return cuda_fail(e, "upload");
-  const size_t smem = n <= kSeedSmemPoints ? sizeof(double) * n : 0;
-  if ((e = cudaFuncSetAttribute(kpp_seed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
-    return cuda_fail(e, "k-means++ shared memory");
-  kpp_seed_kernel<<<1, kSeedThreads, smem>>>(d_pts, n, K, first, d_prob, d_mind, d_cent);
+  if (n <= kSeedSmemPoints) {
+    const size_t smem = sizeof(double) * n;
+    if ((e = cudaFuncSetAttribute(kpp_seed_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+      return cuda_fail(e, "k-means++ shared memory");
+    kpp_seed_kernel<true><<<1, kSeedThreads, smem>>>(d_pts, n, K, first, d_prob, d_mind, d_cent);
+  } else {
+    kpp_seed_kernel<false><<<1, kSeedThreads, 0>>>(d_pts, n, K, first, d_prob, d_mind, d_cent);
+  }
   if ((e = cudaGetLastError())) return cuda_fail(e, "k-means++ launch");
   const int ablocks = std::min((n + 255) / 256, 148 * 8), ublocks = std::min((K + 7) / 8, 148 * 8);
   for (int it = 0; it < iters; ++it) {
