@@ -16,7 +16,7 @@ from . import _abi
 from ._abi import (SD_PDB_NOH, SD_PDB_NOW, SD_PDB_NOXT, SD_PREC_FP64, SD_PREC_FP64_REF,  # noqa: F401
                    SD_PREC_MIXED, SD_SCORING_DFIRE, SD_SCORING_PYDOCK, SparkleError, check, dptr, iptr)
 
-__all__ = ["SyntheticComplex", "Structure", "synthetic_tables", "synthetic_protein_pdb", "place_swarms", "write_pose_pdb", "gso_draws", "mixed_variant_count", "GsoParams", "Docking",
+__all__ = ["SyntheticComplex", "Structure", "synthetic_tables", "synthetic_protein_pdb", "place_swarms", "write_pose_pdb", "reference_point", "gso_draws", "mixed_variant_count", "GsoParams", "Docking",
            "SD_PREC_FP64_REF", "SD_PREC_FP64", "SD_PREC_MIXED", "SD_SCORING_DFIRE",
            "SD_SCORING_PYDOCK", "SparkleError", "device_count"]
 
@@ -130,6 +130,15 @@ class Structure:
         finally:
             _abi.lib().sd_structure_free(h)
         return modes, xyz, lam
+
+
+def reference_point(xyz) -> np.ndarray:
+    """The ligand reference point (sd_reference_point: Khachiyan minimum-volume enclosing
+    ellipsoid centre, tolerance 0.01) of coordinates [n][3]."""
+    x = np.ascontiguousarray(xyz, np.float64)
+    out = np.empty(3)
+    check(_abi.lib().sd_reference_point(dptr(x), x.shape[0], dptr(out)), "sd_reference_point")
+    return out
 
 
 def write_pose_pdb(path, receptor: Structure, rec_xyz, ligand: Structure = None, lig_xyz=None) -> None:

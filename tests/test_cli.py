@@ -111,9 +111,7 @@ def test_cli_pdb_inputs_match_oracle(tmp_path, tables):
     _, poses = sd.place_swarms(rs, ls, S, G, 10, 10, True, seed, 324324)
     cx.rec_modes[:], cx.rec_xyz[:], _ = rs.anm(10, 0.5, S, G)
     cx.lig_modes[:], cx.lig_xyz[:], _ = ls.anm(10, 0.5, S, G)
-    ref = np.empty(3)
-    sd._abi.lib().sd_reference_point(sd.dptr(cx.lig_xyz), ls.n_atoms, sd.dptr(ref))
-    cx.lig_ref = ref
+    cx.lig_ref = sd.reference_point(cx.lig_xyz)
     osys = OracleSystem(cx, tables)
     st = OracleState(S, G, cx.pose_len, poses)
     U = sd.gso_draws(0, S, steps, G)
