@@ -30,8 +30,9 @@ namespace {
 constexpr int kPdWarps = 4;
 constexpr double kKe = 332.0636 / 4.0;
 
+// the switch with its constant 1 / (off2 - on2)^3 passed in (both widths are fixed)
 template <class T>
-__device__ __forceinline__ void pd_switch(T x, T on2, T off2, T& s, T& ds) {
+__device__ __forceinline__ void pd_switch(T x, T on2, T off2, T rden, T& s, T& ds) {
   if (x <= on2) {
     s = T(1);
     ds = T(0);
@@ -42,29 +43,29 @@ __device__ __forceinline__ void pd_switch(T x, T on2, T off2, T& s, T& ds) {
     ds = T(0);
     return;
   }
-  const T w = off2 - on2;
-  const T den = w * w * w;
-  s = (off2 - x) * (off2 - x) * (off2 + T(2) * x - T(3) * on2) / den;
-  ds = T(6) * (off2 - x) * (on2 - x) / den;
+  const T a = off2 - x;
+  s = a * a * (off2 + T(2) * x - T(3) * on2) * rden;
+  ds = T(6) * a * (on2 - x) * rden;
 }
 
-// pair energy and dE/dx for x < 225
+// pair energy and dE/dx for x < 225; two divisions per pair (1 / (x + 1) and, inside 8 A,
+// 1 / (x + sig2 / 2)), every other quotient a product with them
 template <class T>
 __device__ __forceinline__ T pd_pair(T x, T qq, T eps, T sig2, T& dedx) {
   T s, ds;
   const T inv = T(1) / (x + T(1));
   const T el = qq * inv;
-  pd_switch<T>(x, T(196), T(225), s, ds);
+  pd_switch<T>(x, T(196), T(225), T(1) / T(24389), s, ds);  // (225 - 196)^3
   T e = el * s;
   T de = -el * inv * s + el * ds;
   if (x < T(64)) {
-    const T den = x + T(0.5) * sig2;
-    const T sv = sig2 / den;
-    const T s3 = sv * sv * sv, s6 = s3 * s3;
+    const T rden = T(1) / (x + T(0.5) * sig2);
+    const T sv = sig2 * rden;
+    const T s2 = sv * sv, s3 = s2 * sv, s6 = s3 * s3;
     const T lj = T(4) * eps * (s6 - s3);
-    const T dsv = -sv / den;
-    const T dlj = T(4) * eps * (T(6) * s6 / sv - T(3) * s3 / sv) * dsv;
-    pd_switch<T>(x, T(49), T(64), s, ds);
+    const T dsv = -sv * rden;
+    const T dlj = T(4) * eps * (T(6) * s3 * s2 - T(3) * s2) * dsv;  // d(s^6 - s^3)/ds = 6 s^5 - 3 s^2
+    pd_switch<T>(x, T(49), T(64), T(1) / T(3375), s, ds);  // (64 - 49)^3
     e += T(0.1) * (lj * s);
     de += T(0.1) * (dlj * s + lj * ds);
   }
