@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(kPdWarps * 32) pydock_kernel(ScoreLaunch L, do
     }
     __syncthreads();
     const int ntile = sh_ntile;
-    T es = T(0), ec = T(0);  // energy (compensated in FP32)
+    double es = 0.0;  // energy: FP64 per-lane sum of the pair terms
     T grec[SD_MAX_MODES];
     for (int m = 0; m < SD_MAX_MODES; ++m) grec[m] = T(0);
 
@@ -255,14 +255,7 @@ __global__ void __launch_bounds__(kPdWarps * 32) pydock_kernel(ScoreLaunch L, do
               T dedx;
               const int ij = rlj + llj[s];
               const T e = pd_pair<T>(x, rq * lq[s], sh_eps[ij], sh_sig2[ij], dedx);
-              if (sizeof(T) == 4) {
-                const T y = e - ec;
-                const T t = es + y;
-                ec = (t - es) - y;
-                es = t;
-              } else {
-                es += e;
-              }
+              es += (double)e;
               if (GRAD) {
                 const T g2 = T(2) * dedx;
                 gx += g2 * dx;
@@ -297,7 +290,7 @@ __global__ void __launch_bounds__(kPdWarps * 32) pydock_kernel(ScoreLaunch L, do
     // pose results: energy (and gradient) reduced in FP64 over the block
     double acc[1 + 6 + 2 * SD_MAX_MODES];
     const int ng = GRAD ? 6 + C.nmr + C.nml : 0;
-    acc[0] = (double)es - (double)ec;
+    acc[0] = es;
     if (GRAD) {
       for (int k = 1; k <= ng; ++k) acc[k] = 0.0;
       for (int m = 0; m < C.nmr; ++m) acc[1 + 6 + m] = (double)grec[m];
