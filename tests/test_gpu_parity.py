@@ -76,6 +76,39 @@ def test_gso_trajectory_fp64_bit_exact(c0, tables):
     assert stats["guard_errors"] == 0
 
 
+@pytest.mark.parametrize("precision", [sd.SD_PREC_FP64, sd.SD_PREC_MIXED])
+def test_gso_without_modes(precision, tables):
+    """A run without ANM (use_anm false: 0 + 0 modes, 7-element poses): FP64 state bit-identical to
+    the oracle's every step; mixed scores within the bar and its GSO update bit-identical when fed
+    the GPU's own scores."""
+    cx = sd.SyntheticComplex(757, 481, 2, 100, n_modes_rec=0, n_modes_lig=0, seed=91)
+    assert cx.pose_len == 7
+    steps = 10
+    U = sd.gso_draws(3, cx.n_swarms, steps, cx.n_glowworms)
+    osys = OracleSystem(cx, tables)
+    st = OracleState(cx.n_swarms, cx.n_glowworms, cx.pose_len, cx.poses)
+    with sd.Docking([cx], tables, precision=precision) as dk:
+        dk.init_state(0, cx.poses)
+        dk.set_draws(0, U)
+        for t in range(steps):
+            if precision == sd.SD_PREC_FP64:
+                oracle_step(osys, st, U[:, t, :])
+                dk.step(1)
+                g = dk.get_state(0)
+            else:
+                rescored = (st.moved == 1) | (st.step == 0)
+                free = st.copy()
+                oracle_step(osys, free, U[:, t, :])
+                dk.step(1)
+                g = dk.get_state(0)
+                if rescored.any():
+                    assert rel_err(g.scoring[rescored], free.scoring[rescored]).max() <= MIXED_TOL
+                oracle_step(osys, st, U[:, t, :], score_override=g.scoring)
+            for f, o in STATE_FIELDS:
+                assert np.array_equal(getattr(g, f), getattr(st, o)), f"step {t}: {f} differs"
+        assert dk.stats()["guard_errors"] == 0
+
+
 def test_gso_step_locked_mixed(c0, tables):
     steps = 12
     U = sd.gso_draws(1, c0.n_swarms, steps, c0.n_glowworms)
