@@ -16,7 +16,8 @@ from . import _abi
 from ._abi import (SD_PDB_NOH, SD_PDB_NOW, SD_PDB_NOXT, SD_PREC_FP64, SD_PREC_FP64_REF,  # noqa: F401
                    SD_PREC_MIXED, SD_SCORING_DFIRE, SD_SCORING_PYDOCK, SparkleError, check, dptr, iptr)
 
-__all__ = ["SyntheticComplex", "Structure", "synthetic_tables", "synthetic_protein_pdb", "place_swarms", "write_pose_pdb", "reference_point", "gso_draws", "mixed_variant_count", "GsoParams", "Docking",
+__all__ = ["SyntheticComplex", "Structure", "synthetic_tables", "synthetic_protein_pdb", "place_swarms",
+           "write_pose_pdb", "reference_point", "write_checkpoint", "read_checkpoint", "gso_draws", "mixed_variant_count", "GsoParams", "Docking",
            "SD_PREC_FP64_REF", "SD_PREC_FP64", "SD_PREC_MIXED", "SD_SCORING_DFIRE",
            "SD_SCORING_PYDOCK", "SparkleError", "device_count"]
 
@@ -218,6 +219,26 @@ class State:
 
     def copy(self) -> "State":
         return State(*(np.array(getattr(self, f)) for f in self.__dataclass_fields__))
+
+
+def write_checkpoint(path, state: State, steps_done: int) -> None:
+    """Write a GSO state and the number of steps taken to a checkpoint file (sd_write_checkpoint)."""
+    S, G, pl = state.pos.shape
+    cs = state.as_c()
+    check(_abi.lib().sd_write_checkpoint(str(path).encode(), S, G, pl, steps_done, C.byref(cs)),
+          "sd_write_checkpoint")
+
+
+def read_checkpoint(path):
+    """(State, steps_done) from a checkpoint file (sd_read_checkpoint)."""
+    S, G, pl, steps = C.c_int(), C.c_int(), C.c_int(), C.c_longlong()
+    check(_abi.lib().sd_checkpoint_info(str(path).encode(), C.byref(S), C.byref(G), C.byref(pl), C.byref(steps)),
+          "sd_checkpoint_info")
+    st = State.empty(S.value, G.value, pl.value)
+    cs = st.as_c()
+    check(_abi.lib().sd_read_checkpoint(str(path).encode(), S.value, G.value, pl.value, C.byref(steps),
+                                        C.byref(cs)), "sd_read_checkpoint")
+    return st, steps.value
 
 
 class Docking:

@@ -74,6 +74,7 @@ __global__ void hessian_diag_kernel(const double* xyz, int n, double cutoff2, do
 
 extern "C" int sd_anm(const sd_structure* s, int n_modes, double rmsd, int n_swarms, int n_glowworms, int device,
                       double* modes_out, double* xyz_out, double* eigvals_out) {
+  sd::NvtxRange nvtx_range("sd_anm");
   using namespace sd;
   if (!s || n_modes <= 0 || !(rmsd > 0) || n_swarms <= 0 || n_glowworms <= 0 || !modes_out)
     return fail(SD_ERR_ARG, "sd_anm: bad arguments");

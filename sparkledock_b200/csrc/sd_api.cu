@@ -641,6 +641,7 @@ int sd_device_count(int* n) {
 
 int sd_ctx_create(const sd_complex_desc* complexes, int n_complexes, const sd_tables* tables,
                   const sd_gso_params* params, int scoring, int precision, int device, sd_ctx** out) {
+  sd::NvtxRange nvtx_range("sd_ctx_create");
   if (!out) return fail(SD_ERR_ARG, "sd_ctx_create: out is NULL");
   *out = nullptr;
   if (!complexes || n_complexes <= 0 || n_complexes > SD_MAX_COMPLEX)
@@ -903,6 +904,7 @@ int sd_set_draws(sd_ctx* c, int ci, const double* u, int n_steps) {
 }
 
 int sd_step(sd_ctx* c, int n_steps, int sync) {
+  sd::NvtxRange nvtx_range("sd_step");
   if (!c || n_steps < 0) return fail(SD_ERR_ARG, "sd_step: bad arguments");
   SD_CUDA(cudaSetDevice(c->device));
   for (auto& h : c->cx) {
@@ -985,6 +987,7 @@ int sd_set_precision(sd_ctx* c, int precision) {
 
 int sd_score_poses(sd_ctx* c, int ci, const double* poses, int n, int precision, double* score_out,
                    double* energy_out) {
+  sd::NvtxRange nvtx_range("sd_score_poses");
   if (!c || !poses || !score_out || n < 0 || ci < 0 || ci >= c->ncplx)
     return fail(SD_ERR_ARG, "sd_score_poses: bad arguments");
   if (precision < SD_PREC_FP64_REF || precision > SD_PREC_MIXED)
@@ -1040,6 +1043,7 @@ int sd_score_poses(sd_ctx* c, int ci, const double* poses, int n, int precision,
 }
 
 int sd_dfire_bins(sd_ctx* c, int ci, const double* pose, int precision, int* bins_out) {
+  sd::NvtxRange nvtx_range("sd_dfire_bins");
   if (!c || !pose || !bins_out || ci < 0 || ci >= c->ncplx) return fail(SD_ERR_ARG, "sd_dfire_bins: bad arguments");
   SD_CUDA(cudaSetDevice(c->device));
   const DevComplex& D = c->cx[ci].d;
@@ -1060,6 +1064,7 @@ int sd_dfire_bins(sd_ctx* c, int ci, const double* pose, int precision, int* bin
 
 int sd_pydock_grad(sd_ctx* c, int ci, const double* poses, int n, int precision, double* energy_out,
                    double* grad_out) {
+  sd::NvtxRange nvtx_range("sd_pydock_grad");
   if (!c || !poses || !grad_out || n < 0 || ci < 0 || ci >= c->ncplx)
     return fail(SD_ERR_ARG, "sd_pydock_grad: bad arguments");
   if (c->scoring != SD_SCORING_PYDOCK) return fail(SD_ERR_ARG, "sd_pydock_grad: context scoring is not pyDock");
@@ -1122,6 +1127,7 @@ int sd_pydock_grad(sd_ctx* c, int ci, const double* poses, int n, int precision,
 
 int sd_refine_poses(sd_ctx* c, int ci, double* poses, int n, int iters, double step, int precision,
                     double* energy_before, double* energy_after) {
+  sd::NvtxRange nvtx_range("sd_refine_poses");
   if (!c || !poses || n < 0 || iters < 0 || !(step > 0) || ci < 0 || ci >= c->ncplx)
     return fail(SD_ERR_ARG, "sd_refine_poses: bad arguments");
   if (c->scoring != SD_SCORING_PYDOCK) return fail(SD_ERR_ARG, "sd_refine_poses: context scoring is not pyDock");
@@ -1179,6 +1185,7 @@ int sd_refine_poses(sd_ctx* c, int ci, double* poses, int n, int iters, double s
 }
 
 int sd_materialise_poses(sd_ctx* c, int ci, const int* poses, int n, double* rec_xyz_out, double* lig_xyz_out) {
+  sd::NvtxRange nvtx_range("sd_materialise_poses");
   if (!c || ci < 0 || ci >= c->ncplx || !poses || n <= 0 || (!rec_xyz_out && !lig_xyz_out))
     return fail(SD_ERR_ARG, "sd_materialise_poses: bad arguments");
   if (!c->cx[ci].state_set) return fail(SD_ERR_STATE, "sd_materialise_poses: no state");
@@ -1237,6 +1244,7 @@ int sd_materialise_poses(sd_ctx* c, int ci, const int* poses, int n, double* rec
 
 int sd_cluster(sd_ctx* c, int ci, const int* rec_backbone, const int* lig_backbone, int* n_clusters,
                int* cluster_rep, int* cluster_len, int* member_of) {
+  sd::NvtxRange nvtx_range("sd_cluster");
   if (!c || ci < 0 || ci >= c->ncplx || !rec_backbone || !lig_backbone || !n_clusters || !cluster_rep ||
       !cluster_len || !member_of)
     return fail(SD_ERR_ARG, "sd_cluster: bad arguments");

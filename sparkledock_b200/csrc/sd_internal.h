@@ -5,6 +5,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/sparkle_b200.h"
 
 #if defined(__CUDACC__)
@@ -28,6 +30,15 @@
 #define SD_NOALLOC_SCRATCH_BYTES (288 * 1024) /* its file-scope device scratch array */
 
 namespace sd {
+
+// a named NVTX range over a scope: the entry points show up by name on a profiler's timeline
+// (no cost when no profiler is attached)
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // thread-local error message; returns code
 int fail(int code, const std::string& msg);

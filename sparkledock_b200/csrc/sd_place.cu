@@ -351,6 +351,7 @@ void sample_start_poses(const double* centres, int S, int G, int nmr, int nml, b
 extern "C" int sd_place_swarms(const sd_structure* receptor, const sd_structure* ligand, int n_swarms, int n_glowworms,
                                int n_modes_rec, int n_modes_lig, int use_anm, int starting_points_seed, int anm_seed,
                                double swarm_radius, int rank, int device, double* centers_out, double* poses_out) {
+  sd::NvtxRange nvtx_range("sd_place_swarms");
   using namespace sd;
   if (!receptor || !ligand || n_swarms <= 0 || n_glowworms <= 0 || n_modes_rec < 0 || n_modes_lig < 0 || rank < 0 ||
       !(swarm_radius > 0) || (!centers_out && !poses_out))
