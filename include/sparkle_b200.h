@@ -315,17 +315,19 @@ int sd_write_gso_output(const char* dir, int swarm_offset, int n_swarms, int n_g
 
 /* Checkpoints of one complex's GSO state, so that a long run can stop and resume (no counterpart
  * in the reference, which writes only its final files).  A versioned binary file of the sizes, the
- * number of GSO steps taken (the caller's count) and every field of sd_swarm_state, ending in a
+ * number of GSO steps taken and the number the run was started with (the caller's counts; the
+ * reference's draws [S][STEPS][G] depend on the latter), every field of sd_swarm_state, and a
  * 64-bit FNV-1a hash; it is written under a temporary name and renamed when complete.  Resume:
  * sd_read_checkpoint, sd_set_state, then sd_set_draws with the draws of the remaining steps
- * (u[s][t][g] for t >= steps_done of the run's sd_gso_draws): the trajectory continues as if
+ * (u[s][t][g] for t >= steps_done of the same run's sd_gso_draws): the trajectory continues as if
  * uninterrupted.  sd_read_checkpoint fails on other sizes, a truncated or a corrupted file. Host
- * only; every field pointer of st is required. */
+ * only; every field pointer of st is required; steps_done / steps_total outputs may be NULL. */
 int sd_write_checkpoint(const char* path, int n_swarms, int n_glowworms, int pose_len, long long steps_done,
-                        const sd_swarm_state* st);
+                        long long steps_total, const sd_swarm_state* st);
 int sd_read_checkpoint(const char* path, int n_swarms, int n_glowworms, int pose_len, long long* steps_done,
-                       sd_swarm_state* st);
-int sd_checkpoint_info(const char* path, int* n_swarms, int* n_glowworms, int* pose_len, long long* steps_done);
+                       long long* steps_total, sd_swarm_state* st);
+int sd_checkpoint_info(const char* path, int* n_swarms, int* n_glowworms, int* pose_len, long long* steps_done,
+                       long long* steps_total);
 
 /* Optional post-GSO local refinement (pyDock-scoring contexts; project-defined, no reference
  * counterpart): `iters` steepest-descent steps on the smooth elec + LJ energy using the GPU

@@ -221,24 +221,25 @@ class State:
         return State(*(np.array(getattr(self, f)) for f in self.__dataclass_fields__))
 
 
-def write_checkpoint(path, state: State, steps_done: int) -> None:
-    """Write a GSO state and the number of steps taken to a checkpoint file (sd_write_checkpoint)."""
+def write_checkpoint(path, state: State, steps_done: int, steps_total: int = 0) -> None:
+    """Write a GSO state, the steps taken and the steps the run was started with (0: not given) to
+    a checkpoint file (sd_write_checkpoint)."""
     S, G, pl = state.pos.shape
     cs = state.as_c()
-    check(_abi.lib().sd_write_checkpoint(str(path).encode(), S, G, pl, steps_done, C.byref(cs)),
+    check(_abi.lib().sd_write_checkpoint(str(path).encode(), S, G, pl, steps_done, steps_total, C.byref(cs)),
           "sd_write_checkpoint")
 
 
 def read_checkpoint(path):
-    """(State, steps_done) from a checkpoint file (sd_read_checkpoint)."""
-    S, G, pl, steps = C.c_int(), C.c_int(), C.c_int(), C.c_longlong()
-    check(_abi.lib().sd_checkpoint_info(str(path).encode(), C.byref(S), C.byref(G), C.byref(pl), C.byref(steps)),
-          "sd_checkpoint_info")
+    """(State, steps_done, steps_total) from a checkpoint file (sd_read_checkpoint)."""
+    S, G, pl, done, total = C.c_int(), C.c_int(), C.c_int(), C.c_longlong(), C.c_longlong()
+    check(_abi.lib().sd_checkpoint_info(str(path).encode(), C.byref(S), C.byref(G), C.byref(pl), C.byref(done),
+                                        C.byref(total)), "sd_checkpoint_info")
     st = State.empty(S.value, G.value, pl.value)
     cs = st.as_c()
-    check(_abi.lib().sd_read_checkpoint(str(path).encode(), S.value, G.value, pl.value, C.byref(steps),
-                                        C.byref(cs)), "sd_read_checkpoint")
-    return st, steps.value
+    check(_abi.lib().sd_read_checkpoint(str(path).encode(), S.value, G.value, pl.value, C.byref(done),
+                                        C.byref(total), C.byref(cs)), "sd_read_checkpoint")
+    return st, done.value, total.value
 
 
 class Docking:

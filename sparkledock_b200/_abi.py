@@ -104,10 +104,11 @@ SIGNATURES = {
     "sd_structure_arrays": (C.c_int, [C.c_void_p, _dp, _ip, _ip, _ip, _dp]),
     "sd_structure_free": (C.c_int, [C.c_void_p]),
     "sd_write_pose_pdb": (C.c_int, [C.c_char_p, C.c_void_p, _dp, C.c_void_p, _dp]),
-    "sd_write_checkpoint": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_longlong, C.POINTER(SwarmState)]),
+    "sd_write_checkpoint": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_longlong, C.c_longlong,
+                                      C.POINTER(SwarmState)]),
     "sd_read_checkpoint": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_longlong),
-                                     C.POINTER(SwarmState)]),
-    "sd_checkpoint_info": (C.c_int, [C.c_char_p, _ip, _ip, _ip, C.POINTER(C.c_longlong)]),
+                                     C.POINTER(C.c_longlong), C.POINTER(SwarmState)]),
+    "sd_checkpoint_info": (C.c_int, [C.c_char_p, _ip, _ip, _ip, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "sd_materialise_poses": (C.c_int, [C.c_void_p, C.c_int, _ip, C.c_int, _dp, _dp]),
     "sd_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
     "sd_score_poses": (C.c_int, [C.c_void_p, C.c_int, _dp, C.c_int, C.c_int, _dp, _dp]),

@@ -18,6 +18,10 @@
 //        refused (the reference leaves them undeveloped); pyDock charges are seeded stand-ins
 //   "synthetic": {"receptor_atoms": N, "ligand_atoms": M, "seed": s}
 //        seeded synthetic receptor/ligand in place of receptor_pdb / ligand_pdb
+//   "checkpoint_every": N   write <dir>/checkpoint.ckpt (sd_write_checkpoint) every N steps and
+//        at the end.  -t STOP runs only the first STOP of the -s steps and writes the checkpoint
+//        (a segment of the run; no result files); -r CHECKPOINT resumes from a checkpoint of the
+//        same setup.json and -s (the reference's draws depend on -s: other values are refused)
 //   "dfire_table": path of a DCparams-format file (168*168*20 values, one per line);
 //        absent: seeded synthetic table ("table_seed", default 3)
 // -s STEPS is honoured (the reference parses it but runs its compiled STEPS macro).
@@ -199,18 +203,22 @@ int die(const std::string& m) {
 int main(int argc, char** argv) {
   std::string file;
   int steps = 100;  // the reference's STEPS on its GPU path
-  std::string outdir = ".";
-  int device = 0;
+  std::string outdir = ".", resume;
+  int device = 0, stop_at = -1;
   int ch;
-  while ((ch = getopt(argc, argv, "f:s:l:o:d:")) != -1) {
+  const char* usage =
+      "usage: lightdock_b200 -f setup.json [-s STEPS] [-o DIR] [-d DEVICE] [-t STOP] [-r CHECKPOINT]";
+  while ((ch = getopt(argc, argv, "f:s:l:o:d:r:t:")) != -1) {
     if (ch == 'f') file = optarg;
     else if (ch == 's') steps = atoi(optarg);
     else if (ch == 'l') (void)atoi(optarg);  // parsed and unused, as in the reference
     else if (ch == 'o') outdir = optarg;
     else if (ch == 'd') device = atoi(optarg);
-    else return die("usage: lightdock_b200 -f setup.json [-s STEPS] [-o DIR] [-d DEVICE]");
+    else if (ch == 'r') resume = optarg;
+    else if (ch == 't') stop_at = atoi(optarg);
+    else return die(usage);
   }
-  if (file.empty()) return die("usage: lightdock_b200 -f setup.json [-s STEPS] [-o DIR] [-d DEVICE]");
+  if (file.empty()) return die(usage);
   if (steps <= 0) return die("-s STEPS must be positive");
   std::ifstream in(file);
   if (!in) return die("cannot open " + file);
@@ -233,6 +241,7 @@ int main(int argc, char** argv) {
   int precision = prec_s == "mixed" ? SD_PREC_MIXED : prec_s == "fp64" ? SD_PREC_FP64 : prec_s == "fp64_ref" ? SD_PREC_FP64_REF : -1;
   if (precision < 0) return die("setup.json: \"precision\" must be \"mixed\", \"fp64\" or \"fp64_ref\"");
   std::string write_poses = "none";
+  const int checkpoint_every = (int)num_or(root, "checkpoint_every", 0);
   const JVal* syn = root.get("synthetic");
   const bool pdb_input = !syn || syn->kind != JVal::Obj;
   // PDB inputs: structures read as the reference's setup reads them (flags noxt / noh / now)
@@ -345,11 +354,63 @@ int main(int argc, char** argv) {
   const auto t0 = std::chrono::steady_clock::now();
   std::vector<double> u((size_t)swarms * steps * G);
   sd_gso_draws(0, swarms, steps, G, u.data());  // the reference CPU path's serial mt19937(0)
-  int rc = sd_init_state(ctx, 0, pos0);
-  if (!rc) rc = sd_set_draws(ctx, 0, u.data(), steps);
-  if (!rc) rc = sd_step(ctx, steps, 1);
   const int pl = SD_POSE_LEN(anm_rec, anm_lig);
   const size_t n = (size_t)swarms * G;
+  // the whole state, for checkpoints: written to <dir>/checkpoint.ckpt every checkpoint_every steps
+  // and at the end; -r resumes from one (same setup), running the remaining steps with their draws
+  std::vector<double> kpos(n * pl), ksc(n), kluc(n), kvis(n), kref(n * 3);
+  std::vector<int> kstep(n), kmoved(n), knnei(n), ksel(n);
+  sd_swarm_state ks = {kpos.data(), ksc.data(), kluc.data(), kvis.data(), kstep.data(),
+                       kmoved.data(), knnei.data(), ksel.data(), kref.data()};
+  const std::string ckpt_path = (outdir.empty() ? std::string(".") : outdir) + "/checkpoint.ckpt";
+  const long long stop = stop_at >= 0 ? std::min(stop_at, steps) : steps;
+  if ((checkpoint_every > 0 || !resume.empty() || stop < steps) && !outdir.empty() && outdir != "." &&
+      mkdir(outdir.c_str(), 0755) != 0 && errno != EEXIST) {
+    sd_ctx_destroy(ctx);
+    return die("cannot create output directory " + outdir);
+  }
+  long long done = 0;
+  int rc = SD_OK;
+  std::string cli_err;
+  if (!resume.empty()) {
+    long long planned = 0;
+    rc = sd_read_checkpoint(resume.c_str(), swarms, G, pl, &done, &planned, &ks);
+    if (!rc && planned != 0 && planned != steps) {
+      // the reference's draws [S][STEPS][G] differ with STEPS: only the same run continues
+      cli_err = "checkpoint " + resume + " is of a " + std::to_string(planned) + "-step run; give -s " +
+                std::to_string(planned);
+      rc = SD_ERR_ARG;
+    } else if (!rc && done > stop) {
+      cli_err = "checkpoint " + resume + " is past step " + std::to_string(stop);
+      rc = SD_ERR_ARG;
+    }
+    if (!rc) rc = sd_set_state(ctx, 0, &ks);
+  } else {
+    rc = sd_init_state(ctx, 0, pos0);
+  }
+  while (!rc && done < stop) {
+    const int chunk = (int)std::min<long long>(checkpoint_every > 0 ? checkpoint_every : stop, stop - done);
+    std::vector<double> uc((size_t)swarms * chunk * G);  // draws of steps [done, done + chunk)
+    for (int sw = 0; sw < swarms; ++sw)
+      std::copy(u.begin() + ((size_t)sw * steps + done) * G, u.begin() + ((size_t)sw * steps + done + chunk) * G,
+                uc.begin() + (size_t)sw * chunk * G);
+    rc = sd_set_draws(ctx, 0, uc.data(), chunk);
+    if (!rc) rc = sd_step(ctx, chunk, 1);
+    done += chunk;
+    if (!rc && (checkpoint_every > 0 || (done == stop && stop < steps))) {
+      rc = sd_get_state(ctx, 0, &ks);
+      if (!rc) rc = sd_write_checkpoint(ckpt_path.c_str(), swarms, G, pl, done, steps, &ks);
+    }
+  }
+  if (!rc && stop < steps) {  // -t: a segment of the run; the results come with its last segment
+    sd_ctx_destroy(ctx);
+    printf("stopped after step %lld of %d; resume with -r %s\n", done, steps, ckpt_path.c_str());
+    return 0;
+  }
+  if (rc && !cli_err.empty()) {
+    sd_ctx_destroy(ctx);
+    return die(cli_err);
+  }
   std::vector<double> pos(n * pl), luc(n), vis(n), sc(n);
   std::vector<int> nnei(n);
   sd_swarm_state st = {pos.data(), sc.data(), luc.data(), vis.data(), nullptr, nullptr, nnei.data(), nullptr, nullptr};

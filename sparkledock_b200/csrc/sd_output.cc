@@ -93,7 +93,7 @@ extern "C" int sd_write_cluster_repr(const char* dir, int swarm_offset, int n_sw
 
 // ---- checkpoints of one complex's GSO state ----
 // Layout (native byte order): "SDCKPT01", int32 n_swarms, n_glowworms, pose_len, 0, int64
-// steps_done, then pos [S][G][pl], scoring, luciferin, vision_range [S][G] (double), step, moved,
+// steps_done, int64 steps_total, then pos [S][G][pl], scoring, luciferin, vision_range [S][G] (double), step, moved,
 // nnei_len, select [S][G] (int32), ligand_reference_pose [S][G][3] (double), and a trailing FNV-1a
 // 64-bit hash of everything before it.
 namespace {
@@ -130,32 +130,34 @@ bool ckpt_state_complete(const sd_swarm_state* st) {
          st->nnei_len && st->select && st->ligand_reference_pose;
 }
 
-int read_header(std::FILE* f, int dims[4], long long* steps, Fnv& fnv) {
+int read_header(std::FILE* f, int dims[4], long long steps[2], Fnv& fnv) {
   char magic[8];
   if (std::fread(magic, 1, 8, f) != 8 || std::memcmp(magic, kCkptMagic, 8) != 0) return SD_ERR_ARG;
-  if (std::fread(dims, sizeof(int), 4, f) != 4 || std::fread(steps, sizeof(long long), 1, f) != 1) return SD_ERR_ARG;
+  if (std::fread(dims, sizeof(int), 4, f) != 4 || std::fread(steps, sizeof(long long), 2, f) != 2) return SD_ERR_ARG;
   fnv.add(magic, 8);
   fnv.add(dims, sizeof(int) * 4);
-  fnv.add(steps, sizeof(long long));
+  fnv.add(steps, sizeof(long long) * 2);
   return SD_OK;
 }
 
 }  // namespace
 
 extern "C" int sd_write_checkpoint(const char* path, int n_swarms, int n_glowworms, int pose_len, long long steps_done,
-                                   const sd_swarm_state* st) {
-  if (!path || n_swarms <= 0 || n_glowworms <= 0 || pose_len < 7 || steps_done < 0 || !ckpt_state_complete(st))
+                                   long long steps_total, const sd_swarm_state* st) {
+  if (!path || n_swarms <= 0 || n_glowworms <= 0 || pose_len < 7 || steps_done < 0 || steps_total < 0 ||
+      !ckpt_state_complete(st))
     return sd::fail(SD_ERR_ARG, "sd_write_checkpoint: bad arguments");
   const std::string tmp = std::string(path) + ".partial";
   std::FILE* f = std::fopen(tmp.c_str(), "wb");
   if (!f) return sd::fail(SD_ERR_ARG, std::string("sd_write_checkpoint: cannot open ") + tmp);
   Fnv fnv;
   const int dims[4] = {n_swarms, n_glowworms, pose_len, 0};
+  const long long steps[2] = {steps_done, steps_total};
   bool ok = std::fwrite(kCkptMagic, 1, 8, f) == 8 && std::fwrite(dims, sizeof(int), 4, f) == 4 &&
-            std::fwrite(&steps_done, sizeof(long long), 1, f) == 1;
+            std::fwrite(steps, sizeof(long long), 2, f) == 2;
   fnv.add(kCkptMagic, 8);
   fnv.add(dims, sizeof(dims));
-  fnv.add(&steps_done, sizeof(steps_done));
+  fnv.add(steps, sizeof(steps));
   for (const CkptField& c : ckpt_fields(st, n_swarms, n_glowworms, pose_len)) {
     ok = ok && std::fwrite(c.data, 1, c.bytes, f) == c.bytes;
     fnv.add(c.data, c.bytes);
@@ -171,32 +173,33 @@ extern "C" int sd_write_checkpoint(const char* path, int n_swarms, int n_glowwor
 }
 
 extern "C" int sd_checkpoint_info(const char* path, int* n_swarms, int* n_glowworms, int* pose_len,
-                                  long long* steps_done) {
+                                  long long* steps_done, long long* steps_total) {
   if (!path) return sd::fail(SD_ERR_ARG, "sd_checkpoint_info: bad arguments");
   std::FILE* f = std::fopen(path, "rb");
   if (!f) return sd::fail(SD_ERR_ARG, std::string("sd_checkpoint_info: cannot open ") + path);
   int dims[4];
-  long long steps = 0;
+  long long steps[2] = {0, 0};
   Fnv fnv;
-  const int rc = read_header(f, dims, &steps, fnv);
+  const int rc = read_header(f, dims, steps, fnv);
   std::fclose(f);
   if (rc) return sd::fail(rc, std::string("sd_checkpoint_info: not a checkpoint: ") + path);
   if (n_swarms) *n_swarms = dims[0];
   if (n_glowworms) *n_glowworms = dims[1];
   if (pose_len) *pose_len = dims[2];
-  if (steps_done) *steps_done = steps;
+  if (steps_done) *steps_done = steps[0];
+  if (steps_total) *steps_total = steps[1];
   return SD_OK;
 }
 
 extern "C" int sd_read_checkpoint(const char* path, int n_swarms, int n_glowworms, int pose_len, long long* steps_done,
-                                  sd_swarm_state* st) {
+                                  long long* steps_total, sd_swarm_state* st) {
   if (!path || !ckpt_state_complete(st)) return sd::fail(SD_ERR_ARG, "sd_read_checkpoint: bad arguments");
   std::FILE* f = std::fopen(path, "rb");
   if (!f) return sd::fail(SD_ERR_ARG, std::string("sd_read_checkpoint: cannot open ") + path);
   int dims[4];
-  long long steps = 0;
+  long long steps[2] = {0, 0};
   Fnv fnv;
-  if (read_header(f, dims, &steps, fnv)) {
+  if (read_header(f, dims, steps, fnv)) {
     std::fclose(f);
     return sd::fail(SD_ERR_ARG, std::string("sd_read_checkpoint: not a checkpoint: ") + path);
   }
@@ -218,6 +221,7 @@ extern "C" int sd_read_checkpoint(const char* path, int n_swarms, int n_glowworm
   std::fclose(f);
   if (!ok || h != fnv.h)
     return sd::fail(SD_ERR_ARG, std::string("sd_read_checkpoint: truncated or corrupted: ") + path);
-  if (steps_done) *steps_done = steps;
+  if (steps_done) *steps_done = steps[0];
+  if (steps_total) *steps_total = steps[1];
   return SD_OK;
 }

@@ -39,9 +39,9 @@ def _equal(a, b):
 def test_checkpoint_roundtrip(tmp_path):
     st = _random_state(3, 17, 27, 1)
     path = tmp_path / "run.ckpt"
-    sd.write_checkpoint(path, st, 42)
-    back, steps = sd.read_checkpoint(path)
-    assert steps == 42 and _equal(st, back)
+    sd.write_checkpoint(path, st, 42, 100)
+    back, steps, total = sd.read_checkpoint(path)
+    assert steps == 42 and total == 100 and _equal(st, back)
     assert not os.path.exists(str(path) + ".partial")
 
 
@@ -55,7 +55,7 @@ def test_checkpoint_refuses_bad_files(tmp_path):
     other = sd.State.empty(2, 6, 7)
     cs = other.as_c()
     steps = sd.C.c_longlong()
-    assert lib.sd_read_checkpoint(str(path).encode(), 2, 6, 7, sd.C.byref(steps), sd.C.byref(cs)) != 0
+    assert lib.sd_read_checkpoint(str(path).encode(), 2, 6, 7, sd.C.byref(steps), None, sd.C.byref(cs)) != 0
     assert "sizes" in sd._abi.lib().sd_last_error().decode()
     # truncated, corrupted, extended, foreign
     for name, data in (("trunc", raw[:-9]), ("flip", raw[:40] + bytes([raw[40] ^ 1]) + raw[41:]),
@@ -82,9 +82,9 @@ def test_resume_from_checkpoint_is_bit_exact(tmp_path, tables):
         dk.init_state(0, cx.poses)
         dk.set_draws(0, U[:, :stop, :])
         dk.step(stop)
-        sd.write_checkpoint(tmp_path / "run.ckpt", dk.get_state(0), stop)
-    st, done = sd.read_checkpoint(tmp_path / "run.ckpt")
-    assert done == stop
+        sd.write_checkpoint(tmp_path / "run.ckpt", dk.get_state(0), stop, steps)
+    st, done, total = sd.read_checkpoint(tmp_path / "run.ckpt")
+    assert done == stop and total == steps
     with sd.Docking([cx], tables, precision=sd.SD_PREC_FP64) as dk:
         dk.set_state(0, st)
         dk.set_draws(0, U[:, done:, :])
@@ -102,8 +102,8 @@ def test_mixed_state_restores_exactly(tmp_path, tables):
         dk.set_draws(0, U[:, :3, :])
         dk.step(3)
         saved = dk.get_state(0)
-        sd.write_checkpoint(tmp_path / "m.ckpt", saved, 3)
-    st, done = sd.read_checkpoint(tmp_path / "m.ckpt")
+        sd.write_checkpoint(tmp_path / "m.ckpt", saved, 3, 6)
+    st, done, _ = sd.read_checkpoint(tmp_path / "m.ckpt")
     with sd.Docking([cx], tables, precision=sd.SD_PREC_MIXED) as dk:
         dk.set_state(0, st)
         assert _equal(dk.get_state(0), saved)

@@ -84,6 +84,34 @@ def test_cli_fp64_run_matches_oracle(tmp_path, tables):
 
 
 @pytest.mark.gpu
+def test_cli_checkpoint_and_resume(tmp_path):
+    """checkpoint_every writes checkpoint.ckpt without changing the run; a run stopped with -t and
+    resumed with -r writes the same gso_<steps>.out files as the straight run; a checkpoint of a
+    run with another -s is refused (the draws differ)."""
+    setup = {"swarms": 2, "glowworms": 40, "anm_rec": 10, "anm_lig": 10, "use_anm": True, "precision": "fp64",
+             "scoring": "dfire", "synthetic": {"receptor_atoms": 400, "ligand_atoms": 250, "seed": 13}}
+    (tmp_path / "setup.json").write_text(json.dumps(setup))
+    (tmp_path / "ck.json").write_text(json.dumps({**setup, "checkpoint_every": 2}))
+    r = run(["-f", "setup.json", "-s", "6", "-o", "straight"], cwd=tmp_path)
+    assert r.returncode == 0, r.stderr
+    r = run(["-f", "ck.json", "-s", "6", "-o", "chunked"], cwd=tmp_path)
+    assert r.returncode == 0, r.stderr
+    r = run(["-f", "setup.json", "-s", "6", "-t", "4", "-o", "seg"], cwd=tmp_path)
+    assert r.returncode == 0 and "stopped after step 4 of 6" in r.stdout, r.stderr
+    assert not (tmp_path / "seg" / "swarm_0" / "gso_6.out").exists()
+    _, done, total = sd.read_checkpoint(tmp_path / "seg" / "checkpoint.ckpt")
+    assert (done, total) == (4, 6)
+    r = run(["-f", "setup.json", "-s", "6", "-o", "seg", "-r", "seg/checkpoint.ckpt"], cwd=tmp_path)
+    assert r.returncode == 0, r.stderr
+    for sw in range(2):
+        ref = (tmp_path / "straight" / f"swarm_{sw}" / "gso_6.out").read_text()
+        assert (tmp_path / "chunked" / f"swarm_{sw}" / "gso_6.out").read_text() == ref
+        assert (tmp_path / "seg" / f"swarm_{sw}" / "gso_6.out").read_text() == ref
+    r = run(["-f", "setup.json", "-s", "8", "-o", "other", "-r", "chunked/checkpoint.ckpt"], cwd=tmp_path)
+    assert r.returncode != 0 and "6-step run" in r.stderr
+
+
+@pytest.mark.gpu
 def test_cli_pdb_inputs_match_oracle(tmp_path, tables):
     """PDB inputs through the command line: structures read as the reference's setup reads them,
     swarms placed by sd_place_swarms, ANM modes from sd_anm (which re-centres each structure),
