@@ -25,6 +25,8 @@
 //   "dfire_table": path of a DCparams-format file (168*168*20 values, one per line);
 //        absent: seeded synthetic table ("table_seed", default 3)
 // -s STEPS is honoured (the reference parses it but runs its compiled STEPS macro).
+// <dir>/run.json: the run's counts, timings, the scorer's rare-path counters and, for mixed
+// precision, the autotuned kernel variant.
 // Output: <dir>/swarm_<i>/gso_<STEPS>.out as the reference GPU path writes them; with PDB inputs
 // also <dir>/swarm_<i>/cluster.repr (sd_cluster on the CA / P atoms) and the final poses as
 // <dir>/swarm_<i>/lightdock_<g>.pdb (sd_materialise_poses + sd_write_pose_pdb, the reference
@@ -241,6 +243,7 @@ int main(int argc, char** argv) {
   int precision = prec_s == "mixed" ? SD_PREC_MIXED : prec_s == "fp64" ? SD_PREC_FP64 : prec_s == "fp64_ref" ? SD_PREC_FP64_REF : -1;
   if (precision < 0) return die("setup.json: \"precision\" must be \"mixed\", \"fp64\" or \"fp64_ref\"");
   std::string write_poses = "none";
+  double place_secs = 0, anm_secs = 0;
   const int checkpoint_every = (int)num_or(root, "checkpoint_every", 0);
   const JVal* syn = root.get("synthetic");
   const bool pdb_input = !syn || syn->kind != JVal::Obj;
@@ -319,8 +322,9 @@ int main(int argc, char** argv) {
       return die(sd_last_error());
     if (sd_reference_point(desc.lig_xyz, desc.n_lig, desc.lig_ref_point) != SD_OK) return die(sd_last_error());
     const auto p2 = std::chrono::steady_clock::now();
-    printf("setup: swarm placement %f s, ANM %f s\n", std::chrono::duration<double>(p1 - p0).count(),
-           std::chrono::duration<double>(p2 - p1).count());
+    place_secs = std::chrono::duration<double>(p1 - p0).count();
+    anm_secs = std::chrono::duration<double>(p2 - p1).count();
+    printf("setup: swarm placement %f s, ANM %f s\n", place_secs, anm_secs);
   }
 
   const size_t tsz = (size_t)SD_DFIRE_TYPES * SD_DFIRE_TYPES * SD_DFIRE_BINS;
@@ -369,7 +373,7 @@ int main(int argc, char** argv) {
     sd_ctx_destroy(ctx);
     return die("cannot create output directory " + outdir);
   }
-  long long done = 0;
+  long long done = 0, resumed_from = 0;
   int rc = SD_OK;
   std::string cli_err;
   if (!resume.empty()) {
@@ -385,6 +389,7 @@ int main(int argc, char** argv) {
       rc = SD_ERR_ARG;
     }
     if (!rc) rc = sd_set_state(ctx, 0, &ks);
+    resumed_from = done;
   } else {
     rc = sd_init_state(ctx, 0, pos0);
   }
@@ -494,7 +499,29 @@ int main(int argc, char** argv) {
     }
     pose_secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
   }
+  int tv = -1, tw = 0, tb = 0;
+  sd_get_tuning(ctx, &tv, &tw, &tb, nullptr, 0);
   sd_ctx_destroy(ctx);
+  // the run's figures as one JSON object, <dir>/run.json
+  {
+    const std::string path = (outdir.empty() ? std::string(".") : outdir) + "/run.json";
+    FILE* jf = std::fopen(path.c_str(), "w");
+    if (!jf) return die("cannot write " + path);
+    std::fprintf(jf,
+                 "{\"steps\": %d, \"resumed_from_step\": %lld, \"swarms\": %d, \"glowworms\": %d, "
+                 "\"receptor_atoms\": %d, \"ligand_atoms\": %d, \"modes\": [%d, %d], \"scoring\": \"%s\", "
+                 "\"precision\": \"%s\", \"seconds\": {\"placement\": %.6f, \"anm\": %.6f, \"gso\": %.6f, "
+                 "\"clustering\": %.6f, \"pose_files\": %.6f}, \"scored_poses\": %lld, "
+                 "\"scored_poses_per_s\": %.1f, \"pose_files\": %lld, \"mixed_variant\": %d, "
+                 "\"counters\": {\"pairs_in_cutoff\": %lld, \"pairs_fallback\": %lld, \"edge_d2_zero\": %lld, "
+                 "\"edge_d2_cutoff\": %lld, \"edge_u_zero\": %lld, \"edge_shortfall\": %lld}}\n",
+                 steps, resume.empty() ? 0LL : resumed_from, swarms, G, desc.n_rec, desc.n_lig, anm_rec, anm_lig,
+                 scoring_s.c_str(), prec_s.c_str(), place_secs, anm_secs, secs, cluster_secs, pose_secs,
+                 stats.scored_poses, stats.scored_poses / secs, pose_files, precision == SD_PREC_MIXED ? tv : -1,
+                 stats.pairs_in_cutoff, stats.pairs_fallback, stats.edge_d2_zero, stats.edge_d2_cutoff,
+                 stats.edge_u_zero, stats.edge_shortfall);
+    std::fclose(jf);
+  }
   printf("simulation execution:%f\n", secs);
   if (pdb_input) printf("clustering: %f s (cluster.repr per swarm)\n", cluster_secs);
   if (pose_files) printf("pose files: %lld lightdock_<g>.pdb in %f s\n", pose_files, pose_secs);

@@ -81,6 +81,9 @@ def test_cli_fp64_run_matches_oracle(tmp_path, tables):
     for s in range(2):
         got = (tmp_path / f"swarm_{s}" / f"gso_{steps}.out").read_text()
         assert got == exp[s]
+    info = json.loads((tmp_path / "run.json").read_text())
+    assert (info["steps"], info["swarms"], info["glowworms"], info["precision"]) == (steps, 2, 40, "fp64")
+    assert info["scored_poses"] >= 80 and info["seconds"]["gso"] > 0 and info["mixed_variant"] == -1
 
 
 @pytest.mark.gpu
