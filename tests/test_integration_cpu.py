@@ -1,4 +1,4 @@
-"""The reference-side bindings shown in INTEGRATION.md (the C++ files a maintainer adds: one in
+"""The reference-side bindings shown in the integration guide (the C++ files a maintainer adds: one in
 place of the reference's GPU translation unit, one in place of its swarm placement and ANM setup
 calls) compile against the reference's own headers and this library's C header, with warnings as
 errors for the bindings themselves."""
