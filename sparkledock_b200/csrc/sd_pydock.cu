@@ -12,7 +12,7 @@
 //   dE/dt = sum_j F_j, dE/dw = sum_j (l_j - t) x F_j, dE/de_lig_m = sum_j mask_j (R M_mj).F_j,
 //   dE/de_rec_m = sum_i mask_i M_mi.G_i, with F_j = dE/dl_j, G_i = dE/dr_i (pair forces).
 //
-// Kernel: one CTA (4 warps) per pose at a time, persistent over a work list; receptor tiles of
+// Kernel: one CTA (8 warps) per pose at a time, persistent over a work list; receptor tiles of
 // 32 (one lane per atom) culled against the ligand sphere and against spatial ligand chunks;
 // per candidate ligand atom every lane evaluates its pair.  GRAD adds per-lane receptor force
 // accumulators (projected onto the receptor modes at the end of each tile) and per-ligand-atom
@@ -27,7 +27,7 @@ namespace sd {
 
 namespace {
 
-constexpr int kPdWarps = 4;
+constexpr int kPdWarps = 8;
 constexpr double kKe = 332.0636 / 4.0;
 
 // the switch with its constant 1 / (off2 - on2)^3 passed in (both widths are fixed)
