@@ -30,6 +30,17 @@ namespace {
 constexpr int kPdWarps = 8;
 constexpr double kKe = 332.0636 / 4.0;
 
+// a ligand atom in shared memory (position relative to t, charge): one 16-byte load in FP32
+template <class T>
+struct alignas(16) LigAtom {
+  T x, y, z, q;
+};
+// the LJ pair parameters of two types, read together
+template <class T>
+struct alignas(2 * sizeof(T)) LjPair {
+  T eps, sig2;
+};
+
 // the switch with its constant 1 / (off2 - on2)^3 passed in (both widths are fixed)
 template <class T>
 __device__ __forceinline__ void pd_switch(T x, T on2, T off2, T rden, T& s, T& ds) {
@@ -88,7 +99,7 @@ __global__ void __launch_bounds__(kPdWarps * 32) pydock_kernel(ScoreLaunch L, do
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double sh_pose[7 + 2 * SD_MAX_MODES];
   __shared__ double sh_q[4], sh_qi[4];
-  __shared__ T sh_eps[SD_LJ_TYPES * SD_LJ_TYPES], sh_sig2[SD_LJ_TYPES * SD_LJ_TYPES];
+  __shared__ LjPair<T> sh_lj[SD_LJ_TYPES * SD_LJ_TYPES];
   __shared__ double sh_red[kPdWarps][32];
   __shared__ float sh_rot[9];
   __shared__ float sh_bound[2];
@@ -97,9 +108,9 @@ __global__ void __launch_bounds__(kPdWarps * 32) pydock_kernel(ScoreLaunch L, do
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int k = tid; k < SD_LJ_TYPES * SD_LJ_TYPES; k += blockDim.x) {
     const int a = k / SD_LJ_TYPES, b = k % SD_LJ_TYPES;
-    sh_eps[k] = (T)sqrt(L.lj_eps[a] * L.lj_eps[b]);
+    sh_lj[k].eps = (T)sqrt(L.lj_eps[a] * L.lj_eps[b]);
     const double sg = 0.5 * (L.lj_sigma[a] + L.lj_sigma[b]);
-    sh_sig2[k] = (T)(sg * sg);
+    sh_lj[k].sig2 = (T)(sg * sg);
   }
   StepCtl* ctl = L.ctl;
   const int parity = ctl->parity;
@@ -152,13 +163,10 @@ __global__ void __launch_bounds__(kPdWarps * 32) pydock_kernel(ScoreLaunch L, do
     __syncthreads();
     const double tx = sh_pose[0], ty = sh_pose[1], tz = sh_pose[2];
     const float dR = sh_bound[0], dL = sh_bound[1];
-    // shared layout: lx, ly, lz, lq [nls] (T), llj [nls] (int), chunk spheres [nlc] (float4),
+    // shared layout: ligand atoms [nls] (LigAtom<T>), llj [nls] (int), chunk spheres [nlc] (float4),
     // tile list [ntiles] (int), GRAD: fx, fy, fz [nls] (T)
-    T* lx = reinterpret_cast<T*>(smem);
-    T* ly = lx + nls;
-    T* lz = ly + nls;
-    T* lq = lz + nls;
-    T* fx = lq + nls;  // GRAD only
+    LigAtom<T>* la = reinterpret_cast<LigAtom<T>*>(smem);
+    T* fx = reinterpret_cast<T*>(la + nls);  // GRAD only
     T* fy = fx + (GRAD ? nls : 0);
     T* fz = fy + (GRAD ? nls : 0);
     float4* chS = reinterpret_cast<float4*>(fz + (GRAD ? nls : 0));
@@ -171,14 +179,10 @@ __global__ void __launch_bounds__(kPdWarps * 32) pydock_kernel(ScoreLaunch L, do
       if (j >= 0) {
         double x, y, z;
         ligand_exact(C, j, sh_pose, sh_q, sh_qi, x, y, z);
-        lx[s] = (T)(x - tx);
-        ly[s] = (T)(y - ty);
-        lz[s] = (T)(z - tz);
-        lq[s] = (T)(kKe * (double)C.l_q[j]);
+        la[s] = LigAtom<T>{(T)(x - tx), (T)(y - ty), (T)(z - tz), (T)(kKe * (double)C.l_q[j])};
         llj[s] = C.l_lj[j];
       } else {
-        lx[s] = ly[s] = lz[s] = (T)1e18;
-        lq[s] = T(0);
+        la[s] = LigAtom<T>{(T)1e18, (T)1e18, (T)1e18, T(0)};
         llj[s] = 0;
       }
       if (GRAD) fx[s] = fy[s] = fz[s] = T(0);
@@ -242,19 +246,22 @@ __global__ void __launch_bounds__(kPdWarps * 32) pydock_kernel(ScoreLaunch L, do
           const int cc = cb + __ffs(cm) - 1;
           cm &= cm - 1;
           const int sb = cc * SD_TILE;
-          const float ax = (float)lx[sb + lane] - cx, ay = (float)ly[sb + lane] - cy, az = (float)lz[sb + lane] - cz;
+          const LigAtom<T> ca = la[sb + lane];
+          const float ax = (float)ca.x - cx, ay = (float)ca.y - cy, az = (float)ca.z - cz;
           unsigned am = __ballot_sync(0xffffffffu, ax * ax + ay * ay + az * az <= reach2);
           while (am) {
             const int b = __ffs(am) - 1;
             am &= am - 1;
             const int s = sb + b;
-            const T dx = rx - lx[s], dy = ry - ly[s], dz = rz - lz[s];
+            const LigAtom<T> a = la[s];
+            const T dx = rx - a.x, dy = ry - a.y, dz = rz - a.z;
             const T x = dx * dx + dy * dy + dz * dz;
             T fxj = T(0), fyj = T(0), fzj = T(0);
             if (x < T(225)) {
               T dedx;
               const int ij = rlj + llj[s];
-              const T e = pd_pair<T>(x, rq * lq[s], sh_eps[ij], sh_sig2[ij], dedx);
+              const LjPair<T> lj = sh_lj[ij];
+              const T e = pd_pair<T>(x, rq * a.q, lj.eps, lj.sig2, dedx);
               es += (double)e;
               if (GRAD) {
                 const T g2 = T(2) * dedx;
@@ -315,7 +322,7 @@ __global__ void __launch_bounds__(kPdWarps * 32) pydock_kernel(ScoreLaunch L, do
         const int j = lorig[s];
         if (j < 0) continue;
         const double Fx = (double)fx[s], Fy = (double)fy[s], Fz = (double)fz[s];
-        const double px = (double)lx[s], py = (double)ly[s], pz = (double)lz[s];  // l_j - t
+        const double px = (double)la[s].x, py = (double)la[s].y, pz = (double)la[s].z;  // l_j - t
         acc[1] += Fx;
         acc[2] += Fy;
         acc[3] += Fz;
