@@ -89,8 +89,17 @@ class SyntheticComplex:
         self.lig_charge = view(d.lig_charge, (n_lig,), np.float64)
         self.rec_lj = view(d.rec_lj_type, (n_rec,), np.int32)
         self.lig_lj = view(d.lig_lj_type, (n_lig,), np.int32)
-        self.lig_ref = np.array(list(d.lig_ref_point), np.float64)
         self.poses = view(poses, (n_swarms, n_glowworms, self.pose_len), np.float64)
+
+    @property
+    def lig_ref(self) -> np.ndarray:
+        """The ligand reference point of the descriptor (a copy; assign to change it)."""
+        return np.array(list(self.desc.lig_ref_point), np.float64)
+
+    @lig_ref.setter
+    def lig_ref(self, v) -> None:
+        for k in range(3):
+            self.desc.lig_ref_point[k] = float(v[k])
 
 
 class Structure:

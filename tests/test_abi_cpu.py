@@ -52,6 +52,9 @@ def test_synthetic_complex_properties():
     assert np.allclose((q ** 2).sum(-1), 1.0)
     again = sd.SyntheticComplex(757, 481, 5, 20, seed=4)
     assert np.array_equal(again.poses, cx.poses) and np.array_equal(again.rec_xyz, cx.rec_xyz)
+    # the reference point is the descriptor's: assigning it changes what a context receives
+    cx.lig_ref = [1.5, -2.0, 3.25]
+    assert list(cx.desc.lig_ref_point) == [1.5, -2.0, 3.25] and np.array_equal(cx.lig_ref, [1.5, -2.0, 3.25])
 
 
 def test_ctx_create_without_gpu_is_a_status_not_a_crash(tables):
