@@ -71,8 +71,8 @@ struct __align__(16) RingBufs {
   float candf[4][64];        // x, y, z, col bits of [buffer][position]: ligand atom centred on t
   __half candh[16][8];       // position pair i: {x(2i), x(2i+1), y.., y.., z.., z.., -w.., -w..}
   float4 rec[32];            // receptor atom of each lane centred on t, row bits
-  int cslot[64];             // [buffer][position]: ligand chunk slot (exact fallback only)
-  int pend[64];              // pending candidate ligand slots
+  unsigned short cslot[64];  // [buffer][position]: ligand chunk slot (exact fallback only)
+  unsigned short pend[64];   // pending candidate ligand slots (below SD_MAX_LIG)
   unsigned short ring[kRingCap];  // (buffer << 10) | (position << 5) | lane
 };
 
@@ -330,7 +330,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
           const float ax = la.x - cx, ay = la.y - cy, az = la.z - cz;
           const bool cand = fmaf(az, az, fmaf(ay, ay, ax * ax)) <= reach2;
           const unsigned am = __ballot_sync(0xffffffffu, cand);
-          if (cand) W.pend[ncand + __popc(am & lt_mask)] = sb + lane;
+          if (cand) W.pend[ncand + __popc(am & lt_mask)] = (unsigned short)(sb + lane);
           ncand += __popc(am);
         }
         const bool exhausted = cm == 0 && cb >= nlc;
@@ -351,7 +351,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
           W.candf[1][par * 32 + pos] = l4.y;
           W.candf[2][par * 32 + pos] = l4.z;
           W.candf[3][par * 32 + pos] = l4.w;
-          W.cslot[par * 32 + pos] = s;
+          W.cslot[par * 32 + pos] = (unsigned short)s;
           if (kH16) {
             // unused place: s = -60000, never in range; loose tile: every place passes
             float lx = 0.f, ly = 0.f, lz = 0.f, nw = tight ? -60000.f : 0.f;
@@ -414,7 +414,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
           int carry = 0;
           if (lane < rest) carry = W.pend[32 + lane];
           __syncwarp();
-          if (lane < rest) W.pend[lane] = carry;
+          if (lane < rest) W.pend[lane] = (unsigned short)carry;
           ncand = rest;
           par ^= 1;
         }
