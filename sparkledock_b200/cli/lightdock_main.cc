@@ -237,6 +237,17 @@ int main(int argc, char** argv) {
   const int anm_rec = use_anm ? (int)num_or(root, "anm_rec", 10) : 0;
   const int anm_lig = use_anm ? (int)num_or(root, "anm_lig", 10) : 0;
   if (swarms <= 0) return die("setup.json: \"swarms\" must be a positive number");
+  // the reference CPU path's serial mt19937(0) draws [S][steps][G], made on a host thread while
+  // the setup below runs (joined before the first step, or on any early return)
+  std::vector<double> u(G > 0 ? (size_t)swarms * steps * G : 0);
+  std::thread draws_thread;
+  if (G > 0) draws_thread = std::thread([&u, swarms, steps, G]() { sd_gso_draws(0, swarms, steps, G, u.data()); });
+  struct Joiner {
+    std::thread& t;
+    ~Joiner() {
+      if (t.joinable()) t.join();
+    }
+  } draws_joiner{draws_thread};
   const std::string scoring_s = str_or(root, "scoring", "dfire"), prec_s = str_or(root, "precision", "mixed");
   int scoring = scoring_s == "dfire" ? SD_SCORING_DFIRE : scoring_s == "pydock" ? SD_SCORING_PYDOCK : -1;
   if (scoring < 0) return die("setup.json: \"scoring\" must be \"dfire\" or \"pydock\"");
@@ -356,8 +367,7 @@ int main(int argc, char** argv) {
   sd_ctx* ctx = nullptr;
   if (sd_ctx_create(&desc, 1, &tables, &p, scoring, precision, device, &ctx) != SD_OK) return die(sd_last_error());
   const auto t0 = std::chrono::steady_clock::now();
-  std::vector<double> u((size_t)swarms * steps * G);
-  sd_gso_draws(0, swarms, steps, G, u.data());  // the reference CPU path's serial mt19937(0)
+  if (draws_thread.joinable()) draws_thread.join();
   const int pl = SD_POSE_LEN(anm_rec, anm_lig);
   const size_t n = (size_t)swarms * G;
   // the whole state, for checkpoints: written to <dir>/checkpoint.ckpt every checkpoint_every steps
