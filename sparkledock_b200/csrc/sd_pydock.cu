@@ -249,18 +249,15 @@ __global__ void __launch_bounds__(kPdWarps * 32) pydock_kernel(ScoreLaunch L, do
           const LigAtom<T> ca = la[sb + lane];
           const float ax = (float)ca.x - cx, ay = (float)ca.y - cy, az = (float)ca.z - cz;
           unsigned am = __ballot_sync(0xffffffffu, ax * ax + ay * ay + az * az <= reach2);
-          while (am) {
-            const int b = __ffs(am) - 1;
-            am &= am - 1;
-            const int s = sb + b;
+          // this lane's pair with candidate slot s: energy, dE/dr_i into (gx, gy, gz), and the
+          // force on the ligand atom into f
+          auto pair = [&](int s, T f[3]) {
             const LigAtom<T> a = la[s];
             const T dx = rx - a.x, dy = ry - a.y, dz = rz - a.z;
             const T x = dx * dx + dy * dy + dz * dz;
-            T fxj = T(0), fyj = T(0), fzj = T(0);
             if (x < T(225)) {
               T dedx;
-              const int ij = rlj + llj[s];
-              const LjPair<T> lj = sh_lj[ij];
+              const LjPair<T> lj = sh_lj[rlj + llj[s]];
               const T e = pd_pair<T>(x, rq * a.q, lj.eps, lj.sig2, dedx);
               es += (double)e;
               if (GRAD) {
@@ -268,19 +265,45 @@ __global__ void __launch_bounds__(kPdWarps * 32) pydock_kernel(ScoreLaunch L, do
                 gx += g2 * dx;
                 gy += g2 * dy;
                 gz += g2 * dz;
-                fxj = -g2 * dx;
-                fyj = -g2 * dy;
-                fzj = -g2 * dz;
+                f[0] = -g2 * dx;
+                f[1] = -g2 * dy;
+                f[2] = -g2 * dz;
               }
             }
-            if (GRAD) {
-              fxj = warp_sum<T>(fxj);
-              fyj = warp_sum<T>(fyj);
-              fzj = warp_sum<T>(fzj);
-              if (lane == 0) {
-                atomicAdd(&fx[s], fxj);
-                atomicAdd(&fy[s], fyj);
-                atomicAdd(&fz[s], fzj);
+          };
+          if (!GRAD) {
+            while (am) {
+              const int b = __ffs(am) - 1;
+              am &= am - 1;
+              T f[3];
+              pair(sb + b, f);
+            }
+          } else {
+            // candidates two at a time: one exchange across the half-warps leaves candidate A's
+            // partial forces in lanes 0-15 and B's in lanes 16-31, four more levels finish both
+            const bool hi = (lane & 16) != 0;
+            while (am) {
+              const int b0 = __ffs(am) - 1;
+              am &= am - 1;
+              int b1 = -1;
+              if (am) {
+                b1 = __ffs(am) - 1;
+                am &= am - 1;
+              }
+              T fa[3] = {T(0), T(0), T(0)}, fb[3] = {T(0), T(0), T(0)};
+              pair(sb + b0, fa);
+              if (b1 >= 0) pair(sb + b1, fb);
+#pragma unroll
+              for (int k = 0; k < 3; ++k) {
+                T v = (hi ? fb[k] : fa[k]) + __shfl_xor_sync(0xffffffffu, hi ? fa[k] : fb[k], 16);
+                for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                fa[k] = v;
+              }
+              const int s = sb + (hi ? b1 : b0);
+              if ((lane & 15) == 0 && (!hi || b1 >= 0)) {
+                atomicAdd(&fx[s], fa[0]);
+                atomicAdd(&fy[s], fa[1]);
+                atomicAdd(&fz[s], fa[2]);
               }
             }
           }
