@@ -279,31 +279,68 @@ __global__ void __launch_bounds__(kPdWarps * 32) pydock_kernel(ScoreLaunch L, do
               pair(sb + b, f);
             }
           } else {
-            // candidates two at a time: one exchange across the half-warps leaves candidate A's
-            // partial forces in lanes 0-15 and B's in lanes 16-31, four more levels finish both
-            const bool hi = (lane & 16) != 0;
-            while (am) {
-              const int b0 = __ffs(am) - 1;
-              am &= am - 1;
-              int b1 = -1;
-              if (am) {
-                b1 = __ffs(am) - 1;
-                am &= am - 1;
-              }
-              T fa[3] = {T(0), T(0), T(0)}, fb[3] = {T(0), T(0), T(0)};
-              pair(sb + b0, fa);
-              if (b1 >= 0) pair(sb + b1, fb);
+            // candidates several at a time share one warp reduction of their ligand forces
+            const bool h16 = (lane & 16) != 0, h8 = (lane & 8) != 0;
+            if constexpr (sizeof(T) == 8) {
+              // FP64 (registers to spare), four: an exchange across the half-warps and one across
+              // the quarter-warps leave candidate A's partial forces in lanes 0-7, B's in 8-15,
+              // C's in 16-23 and D's in 24-31; three more levels finish all four
+              while (am) {
+                int b[4];
 #pragma unroll
-              for (int k = 0; k < 3; ++k) {
-                T v = (hi ? fb[k] : fa[k]) + __shfl_xor_sync(0xffffffffu, hi ? fa[k] : fb[k], 16);
-                for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                fa[k] = v;
+                for (int q = 0; q < 4; ++q) {
+                  b[q] = am ? __ffs(am) - 1 : -1;
+                  if (am) am &= am - 1;
+                }
+                T f[4][3];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                  f[q][0] = f[q][1] = f[q][2] = T(0);
+                  if (b[q] >= 0) pair(sb + b[q], f[q]);
+                }
+                T r[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                  T k0 = h16 ? f[2][k] : f[0][k], k1 = h16 ? f[3][k] : f[1][k];
+                  k0 += __shfl_xor_sync(0xffffffffu, h16 ? f[0][k] : f[2][k], 16);
+                  k1 += __shfl_xor_sync(0xffffffffu, h16 ? f[1][k] : f[3][k], 16);
+                  T v = (h8 ? k1 : k0) + __shfl_xor_sync(0xffffffffu, h8 ? k0 : k1, 8);
+                  for (int o = 4; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                  r[k] = v;
+                }
+                const int bq = b[(h16 ? 2 : 0) + (h8 ? 1 : 0)];
+                if ((lane & 7) == 0 && bq >= 0) {
+                  atomicAdd(&fx[sb + bq], r[0]);
+                  atomicAdd(&fy[sb + bq], r[1]);
+                  atomicAdd(&fz[sb + bq], r[2]);
+                }
               }
-              const int s = sb + (hi ? b1 : b0);
-              if ((lane & 15) == 0 && (!hi || b1 >= 0)) {
-                atomicAdd(&fx[s], fa[0]);
-                atomicAdd(&fy[s], fa[1]);
-                atomicAdd(&fz[s], fa[2]);
+            } else {
+              // FP32, two: one exchange across the half-warps leaves candidate A's partial forces
+              // in lanes 0-15 and B's in 16-31; four more levels finish both
+              while (am) {
+                const int b0 = __ffs(am) - 1;
+                am &= am - 1;
+                int b1 = -1;
+                if (am) {
+                  b1 = __ffs(am) - 1;
+                  am &= am - 1;
+                }
+                T fa[3] = {T(0), T(0), T(0)}, fb[3] = {T(0), T(0), T(0)};
+                pair(sb + b0, fa);
+                if (b1 >= 0) pair(sb + b1, fb);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                  T v = (h16 ? fb[k] : fa[k]) + __shfl_xor_sync(0xffffffffu, h16 ? fa[k] : fb[k], 16);
+                  for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                  fa[k] = v;
+                }
+                const int s = sb + (h16 ? b1 : b0);
+                if ((lane & 15) == 0 && (!h16 || b1 >= 0)) {
+                  atomicAdd(&fx[s], fa[0]);
+                  atomicAdd(&fy[s], fa[1]);
+                  atomicAdd(&fz[s], fa[2]);
+                }
               }
             }
           }
