@@ -64,9 +64,12 @@ __device__ __forceinline__ int exact_key(double d2, const double* T) {
 }
 
 // PREC: SD_PREC_FP64_REF (no culling) or SD_PREC_FP64 (culled); the mixed-precision kernel is
-// in sd_score_mixed.cuh
+// in sd_score_mixed.cuh.  16 warps per CTA: the per-pose shared memory (receptor accumulators,
+// ligand atoms) allows two CTAs per SM, so the warps per CTA set the SM's residency.
+constexpr int kFp64Threads = 512;
+
 template <int PREC>
-__global__ void __launch_bounds__(256) dfire_score_kernel(ScoreLaunch L) {
+__global__ void __launch_bounds__(kFp64Threads) dfire_score_kernel(ScoreLaunch L) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double sh_pose[7 + 2 * SD_MAX_MODES];
   __shared__ double sh_q[4], sh_qi[4];
@@ -309,7 +312,7 @@ int mixed_variant_min_blocks(int v) { return mixed_variant(v).min_blocks; }
 
 int score_threads_of(int precision, int scoring, int variant) {
   if (scoring == SD_SCORING_PYDOCK) return pydock_threads();
-  return precision == SD_PREC_MIXED ? mixed_variant_warps(variant) * 32 : 256;
+  return precision == SD_PREC_MIXED ? mixed_variant_warps(variant) * 32 : kFp64Threads;
 }
 
 const void* score_kernel_ptr(int precision, int scoring, int variant) {
