@@ -29,8 +29,8 @@
 //  * the table is gathered from a key-indexed copy [168][168][32] (entry k is the value the
 //    reference reads for key k, including the d^2 == 225 read of the next ligand type's bin 0),
 //    so no bin lookup is needed; a rejected or padding pair gathers a zero past the table instead
-//    of branching, and each round's gathers are added by the next round, so they are in flight
-//    while the next round is evaluated.  Each lane sums its values in FP64 (Kahan sums of an
+//    of branching, and each round's gathers (through L2 only) are added by the next round, so
+//    they are in flight while the next round is evaluated.  Each lane sums its values in FP64 (Kahan sums of an
 //    FP32-rounded table were measured to miss 1e-5 at 60k pairs per pose); warp shuffles and a
 //    block reduction in FP64 finish the pose.
 //
@@ -403,10 +403,15 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
           const int total = __shfl_sync(0xffffffffu, incl, 31);
           int at = head + incl - cnt;
           const unsigned tag = ((unsigned)par << 10) | (unsigned)lane;
+          // two entries per iteration: the highest and the lowest bit left
           while (m) {
             const int b = 31 - __clz(m);
-            m ^= 1u << b;
-            W.ring[at++] = (unsigned short)(tag | ((unsigned)b << 5));
+            const unsigned low = m & (0u - m);
+            const int b2 = 31 - __clz(low);
+            m &= ~((1u << b) | low);
+            W.ring[at] = (unsigned short)(tag | ((unsigned)b << 5));
+            if (b2 != b) W.ring[at + 1] = (unsigned short)(tag | ((unsigned)b2 << 5));
+            at += b2 != b ? 2 : 1;
           }
           head += total;
           // keep the candidates beyond the first 32
@@ -454,13 +459,15 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
           npairs += ok ? 1u : 0u;
           return ok ? idx : kZeroIdxKey;
         };
+        // the gathers go through L2 only (ld.global.cg): each is used once, and cached in L1 they
+        // would evict the receptor / ligand atom and mode lines that the next tiles read again
         for (int t0 = 0; t0 < upto; t0 += kG) {
           const int n = min(kG, upto - t0);
           acc += pv0;
-          pv0 = __ldg(table + pair(t0, 0, n));
+          pv0 = __ldcg(table + pair(t0, 0, n));
           if (kDual) {
             acc += pv1;
-            pv1 = __ldg(table + pair(t0, 1, n));
+            pv1 = __ldcg(table + pair(t0, 1, n));
           }
         }
         // move the leftover (< kG) entries to the front
