@@ -100,6 +100,13 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def brute_pairs_per_pose(cfg):
+    """Receptor x ligand atom pairs of one pose, averaged over the poses of every complex (each
+    complex weighted by its swarm count: all glowworms of a step are candidates for rescoring)."""
+    cs = cfg["complexes"]
+    return sum(nr * nl * s for nr, nl, s in cs) / sum(s for _, _, s in cs)
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -496,6 +503,17 @@ def main():
             extra[pname] = {"value": sc / (tm / 1e3), "ms_per_step": tm / cmp_steps,
                             "steps_per_s": cmp_steps / (tm / 1e3), "scored_poses": sc, "timed_steps": cmp_steps,
                             "speedup_mixed": ref_value / (sc / (tm / 1e3))}
+            # the same algorithmic work as the mixed line (8 Nr Nl flops per scored pose, or 8 flops
+            # per in-cutoff pair at the mixed run's pairs per pose on the large receptor) over the
+            # nominal FP64 vector pipe: 148 SMs x 64 lanes x 2 at the measured max SM clock
+            fp64_peak = 148 * 64 * 2 * (measured_peaks()[0].get("sm_max_mhz", 1965.0) * 1e6) / 1e12
+            per_pose = (8.0 * brute_pairs_per_pose(cfg) if args.config != "c3" else
+                        8.0 * pairs_all / max(1, scored))
+            ach = per_pose * sc / (tm / 1e3) / 1e12
+            extra[pname]["roofline"] = {"bound": "fp64", "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
+                                        "frac": ach / fp64_peak,
+                                        "peak_source": "nominal FP64 vector pipe (148 SMs x 64 lanes x 2) at the "
+                                                       "measured max SM clock"}
     if args.no_e2e:
         e2e = {"ms": float("nan"), "wall_s": None, "scored": 0, "h2d": 0, "d2h": 0}
     else:
@@ -531,7 +549,7 @@ def main():
                                               "edge_shortfall")},
         "per_scored_pose": {"pairs_in_cutoff": stats["pairs_in_cutoff"] / max(1, stats["scored_poses"]),
                             "pairs_evaluated": stats["pairs_evaluated"] / max(1, stats["scored_poses"]),
-                            "pairs_brute_force": sum(nr * nl for nr, nl, _ in cfg["complexes"]) / len(cfg["complexes"])},
+                            "pairs_brute_force": brute_pairs_per_pose(cfg)},
     }
     if pairs:
         # algorithmic work per scored pose: W = 8 Nr Nl flops (3 sub + 3 mul + 2 add per pair, the
