@@ -30,9 +30,9 @@
 //    reference reads for key k, including the d^2 == 225 read of the next ligand type's bin 0),
 //    so no bin lookup is needed; a rejected or padding pair gathers a zero past the table instead
 //    of branching, and each round's gathers (through L2 only) are added by the next round, so
-//    they are in flight while the next round is evaluated.  Each lane sums its values in FP64 (Kahan sums of an
-//    FP32-rounded table were measured to miss 1e-5 at 60k pairs per pose); warp shuffles and a
-//    block reduction in FP64 finish the pose.
+//    they are in flight while the next round is evaluated.  Each lane sums its values in FP64
+//    (Kahan sums of an FP32-rounded table were measured to miss 1e-5 at 60k pairs per pose);
+//    warp shuffles and a block reduction in FP64 finish the pose.
 //
 // FP16 bound (u = 2^-11, R >= |r - c| for the tile's atoms, Lb >= |l - c| for its candidates,
 // w = |l - c|^2 / 2):  |s_fp16 - (r.l - w)| <= u (2.001 R Lb + w) + 3u (1.002 R Lb + 1.001 w)
@@ -361,11 +361,18 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
               lz = l4.z - cz;
               nw = fmaxf(-0.5f * (lx * lx + ly * ly + lz * lz), -60000.f);
             }
-            __half* q = W.candh[lane >> 1];
-            q[0 + (lane & 1)] = __float2half_rn(lx);
-            q[2 + (lane & 1)] = __float2half_rn(ly);
-            q[4 + (lane & 1)] = __float2half_rn(lz);
-            q[6 + (lane & 1)] = __float2half_rn(nw);
+            // lanes 2i and 2i+1 fill candh[i] with one 8-byte store each: the even lane the x and y
+            // pairs, the odd lane the z and w pairs (conflict-free, where 16-bit stores collide)
+            const __half2 xy = __floats2half2_rn(lx, ly), zw = __floats2half2_rn(lz, nw);
+            const bool odd = lane & 1;
+            const __half2 other = __shfl_xor_sync(0xffffffffu, odd ? xy : zw, 1);
+            const __half2 mine = odd ? zw : xy;
+            const __half2 lo = odd ? other : mine, hi = odd ? mine : other;  // even lane's, odd lane's
+            const __half2 o0 = __lows2half2(lo, hi), o1 = __highs2half2(lo, hi);
+            uint2 u;
+            u.x = reinterpret_cast<const unsigned&>(o0);
+            u.y = reinterpret_cast<const unsigned&>(o1);
+            *reinterpret_cast<uint2*>(reinterpret_cast<unsigned char*>(W.candh[lane >> 1]) + 8 * (lane & 1)) = u;
           }
           __syncwarp();
           // stage 1: bit b of m <=> (this lane's receptor atom, candidate at position b) in range
