@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(kPdWarps * 32) pydock_kernel(ScoreLaunch L, do
         double x, y, z;
         ligand_exact(C, j, sh_pose, sh_q, sh_qi, x, y, z);
         la[s] = LigAtom<T>{(T)(x - tx), (T)(y - ty), (T)(z - tz), (T)(kKe * (double)C.l_q[j])};
-        llj[s] = C.l_lj[j];
+        llj[s] = C.l_lj[j] * SD_LJ_TYPES;
       } else {
         la[s] = LigAtom<T>{(T)1e18, (T)1e18, (T)1e18, T(0)};
         llj[s] = 0;
@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(kPdWarps * 32) pydock_kernel(ScoreLaunch L, do
         ry = (T)(y - ty);
         rz = (T)(z - tz);
         rq = (T)C.r_q[slot];
-        rlj = C.r_lj[slot] * SD_LJ_TYPES;
+        rlj = C.r_lj[slot];
       }
       T gx = T(0), gy = T(0), gz = T(0);  // dE/dr_i
       for (int cb = 0; cb < nlc; cb += 32) {
@@ -257,7 +257,10 @@ __global__ void __launch_bounds__(kPdWarps * 32) pydock_kernel(ScoreLaunch L, do
             const T x = dx * dx + dy * dy + dz * dz;
             if (x < T(225)) {
               T dedx;
-              const LjPair<T> lj = sh_lj[rlj + llj[s]];
+              // the table is symmetric (products and sums of the two types' parameters), so it is
+              // read as [ligand type][receptor type]: the lanes of one candidate read consecutive
+              // entries instead of entries 20 apart that meet in a few banks
+              const LjPair<T> lj = sh_lj[llj[s] + rlj];
               const T e = pd_pair<T>(x, rq * a.q, lj.eps, lj.sig2, dedx);
               es += (double)e;
               if (GRAD) {
