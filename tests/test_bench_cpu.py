@@ -22,3 +22,15 @@ def test_reference_arm_json_line():
     assert d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0
     assert d["cpu_baseline"]["kind"] in ("reference", "port") and d["cpu_baseline"]["cores"] >= 1
     assert d["config"]["workload"]
+
+
+def test_work_per_pose_weighted_by_swarms():
+    """The brute-force work per scored pose averages Nr x Nl over the poses of every complex, so a
+    complex with more swarms counts for more (the batched workload's complexes differ in both)."""
+    sys.path.insert(0, ROOT)
+    import bench
+    cfg = {"complexes": [(100, 10, 1), (1000, 20, 3)]}
+    assert bench.brute_pairs_per_pose(cfg) == (100 * 10 * 1 + 1000 * 20 * 3) / 4
+    c1 = bench.CONFIGS["c1"]
+    nr, nl, _ = c1["complexes"][0]
+    assert bench.brute_pairs_per_pose(c1) == nr * nl
