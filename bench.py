@@ -423,8 +423,9 @@ def main():
     if args.swarms:
         cfg["complexes"] = [(nr, nl, min(s, args.swarms)) for nr, nl, s in cfg["complexes"]]
         cfg["workload"] += f" (swarms capped at {args.swarms})"
-    if args.precision:
+    if args.precision and args.precision != cfg.get("precision"):
         cfg["precision"] = args.precision
+        cfg["workload"] = cfg["workload"].replace("mixed precision", args.precision + " precision")
     rank, world, local = rank_env()
     config = {"workload": cfg["workload"], "complexes": [list(c) for c in cfg["complexes"]], "glowworms": G,
               "anm_modes": [10, 10], "gso_steps": args.warmup + args.steps, "scoring": "dfire",
