@@ -136,6 +136,8 @@ __global__ void __launch_bounds__(kFp64Threads) dfire_score_kernel(ScoreLaunch L
     LigD* ligD = reinterpret_cast<LigD*>(smem + (size_t)16 * ((nl + 1) & ~1));
     double* vacc = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(ligD) + (size_t)32 * nl);
     int* tlist = reinterpret_cast<int*>(vacc + nr);  // tiles within reach of the ligand
+    int* tord = tlist + C.ntiles;                    // the same, closest to t first
+    float* tdist = reinterpret_cast<float*>(tord + C.ntiles);
     if (tid == 0) {
       sh_ntile = 0;
       sh_next = 0;
@@ -169,18 +171,40 @@ __global__ void __launch_bounds__(kFp64Threads) dfire_score_kernel(ScoreLaunch L
                     cz = (float)((double)tile.z - tz);
         const float reach = tile_reach_base + tile.w + lig_reach;
         keep = cx * cx + cy * cy + cz * cz <= reach * reach;
+        if (keep) {
+          const int at = atomicAdd(&sh_ntile, 1);
+          tlist[at] = k;
+          tdist[at] = cx * cx + cy * cy + cz * cz;
+        }
+      } else {
+        tlist[atomicAdd(&sh_ntile, 1)] = k;
       }
-      if (keep) tlist[atomicAdd(&sh_ntile, 1)] = k;
     }
     __syncthreads();
     const int ntile = sh_ntile;
+    // culled: the tiles closest to the ligand centre (t) have the most pairs; taking them first
+    // lets the warps finish a pose together (the tile order does not touch the summation order)
+    const bool sorted = kCull && ntile <= 512;
+    if (sorted) {
+      for (int t = tid; t < ntile; t += blockDim.x) {
+        const float d = tdist[t];
+        int rank = 0;
+        for (int u = 0; u < ntile; ++u) {
+          const float e = tdist[u];
+          rank += (e < d || (e == d && u < t)) ? 1 : 0;
+        }
+        tord[rank] = tlist[t];
+      }
+      __syncthreads();
+    }
+    const int* tl = sorted ? tord : tlist;
 
     for (;;) {
       int ti = 0;
       if (lane == 0) ti = atomicAdd(&sh_next, 1);
       ti = __shfl_sync(0xffffffffu, ti, 0);
       if (ti >= ntile) break;
-      const int k = tlist[ti];
+      const int k = tl[ti];
       const float4 tile = C.r_tile[k];
       const float cx = (float)((double)tile.x - tx), cy = (float)((double)tile.y - ty),
                   cz = (float)((double)tile.z - tz);
@@ -303,7 +327,7 @@ size_t score_smem_bytes(int precision, int scoring, int max_nr, int max_nl, int 
     return (size_t)16 * (nlc * SD_TILE + nlc) + 4 * (3 * ntiles + nlc);
   }
   return (size_t)16 * ((max_nl + 1) & ~1) + (size_t)32 * max_nl + (size_t)8 * max_nr +
-         (size_t)4 * ((max_nr + SD_TILE - 1) / SD_TILE);
+         (size_t)12 * ((max_nr + SD_TILE - 1) / SD_TILE);
 }
 
 int mixed_variant_count() { return kNumMixedVariants; }
