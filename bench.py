@@ -1,12 +1,19 @@
 """Benchmark of the GSO docking step on B200 (scored poses/s and GSO steps/s).
 
 One bench step = one GSO step over every glowworm of the workload (rescore moved poses,
-luciferin, neighbour selection, movement).  Defaults: the mixed-precision single complex
-(receptor 3002 atoms, ligand 1274 atoms, 10+10 ANM modes, 402 swarms x 200 glowworms), 3
-warm-up steps + 97 timed steps = the workload's 100 GSO steps.  The plain FP64 kernels run the
-same steps from the same start for the mixed-vs-FP64 ratio.
+luciferin, neighbour selection, movement).  Default workload: the mixed-precision batched step,
+eight synthetic complexes of uneven sizes (757/481 ... 6143/633 atoms, 130 ... 695 swarms x 200
+glowworms, 640,400 poses, 10+10 ANM modes) in one persistent scorer launch per step, replayed
+from a CUDA graph; 3 warm-up steps + 97 timed steps = the workload's 100 GSO steps.  The plain
+FP64 kernels run the same steps from the same start for the mixed-vs-FP64 ratio.  The same line
+carries the single complex (3002 / 1274 atoms, 402 x 200 glowworms) under "c1", with its own
+ratio and a per-step check of its energies against the plain FP64 kernel.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c1]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2]
+
+--impl reference: the reference's own CPU path (compiled from its sources into oracle/_ref) on a
+bounded sample of the same workload, with inputs from the oracle; the product library is not
+loaded in that process.
 
 N > 1 (torchrun): every rank runs its own replica of the workload on its GPU (the swarms of
 the reference shard with no data exchange); value = all ranks' scored poses / max time.
@@ -115,9 +122,11 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
 
 
-def run_gpu(cfg, prec_name, steps, warmup, device, flush, seed=0, per_step=False):
+def run_gpu(cfg, prec_name, steps, warmup, device, flush, seed=0, per_step=False, energy_every=0):
     """Device-timed run: draws resident in HBM, per-step CUDA events on the context stream,
-    L2 flushed (256 MB write) between timed steps outside the events."""
+    L2 flushed (256 MB write) between timed steps outside the events.  energy_every = k > 0:
+    after every k-th timed step (outside the events) the scores that step wrote for the poses it
+    rescored are checked against the plain FP64 kernel on the same poses (up to 256 per complex)."""
     import torch
     import sparkledock_b200 as sd
     prec = {"mixed": sd.SD_PREC_MIXED, "fp64": sd.SD_PREC_FP64, "fp64_ref": sd.SD_PREC_FP64_REF}[prec_name]
@@ -134,8 +143,11 @@ def run_gpu(cfg, prec_name, steps, warmup, device, flush, seed=0, per_step=False
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
     scored_steps = []
+    energy_err = []
     with torch.cuda.stream(stream):
         for k in range(steps):
+            check = energy_every > 0 and k % energy_every == 0
+            before = [dk.get_state(i) for i in range(len(cxs))] if check else None
             if flush is not None:
                 flush.zero_()
             starts[k].record(stream)
@@ -143,14 +155,39 @@ def run_gpu(cfg, prec_name, steps, warmup, device, flush, seed=0, per_step=False
             ends[k].record(stream)
             if per_step:  # synchronises between steps (outside the timed events)
                 scored_steps.append(dk.stats()["scored_poses"])
+            if check:
+                energy_err.append(step_energy_error(dk, cxs, before, k))
     torch.cuda.synchronize(device)
     ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
     s1 = dk.stats()
     out = {"ms": ms, "scored": s1["scored_poses"] - s0["scored_poses"], "stats": s1, "ctx": dk, "cxs": cxs,
            "pairs": s1["pairs_in_cutoff"] - s0["pairs_in_cutoff"],
            "tuning": dk.tuning(),
-           "per_step": [b - a for a, b in zip([s0["scored_poses"]] + scored_steps, scored_steps)] if per_step else None}
+           "per_step": [b - a for a, b in zip([s0["scored_poses"]] + scored_steps, scored_steps)] if per_step else None,
+           "energy_err": energy_err}
     return out
+
+
+def step_energy_error(dk, cxs, before, k, per_complex=256):
+    """Scores written by one GSO step for the poses it rescored (moved in the step before, or not
+    yet scored), against the plain FP64 kernel on the same poses (the pose each had when the
+    step began): max |s_mixed - s_fp64| / max(|s_fp64|, 1) and the same on the raw DFIRE energy
+    E = (4.7 - s) / 0.0157."""
+    import sparkledock_b200 as sd
+    worst_s, worst_e, n = 0.0, 0.0, 0
+    for i, c in enumerate(cxs):
+        b = before[i]
+        sel = np.flatnonzero(((b.moved == 1) | (b.step == 0)).ravel())
+        if sel.size == 0:
+            continue
+        sel = sel[np.linspace(0, sel.size - 1, min(per_complex, sel.size)).astype(int)]
+        after = dk.get_state(i).scoring.ravel()[sel]
+        s64, e64 = dk.score_poses(i, b.pos.reshape(-1, c.pose_len)[sel], sd.SD_PREC_FP64)
+        worst_s = max(worst_s, float((np.abs(after - s64) / np.maximum(np.abs(s64), 1.0)).max()))
+        e_mixed = (4.7 - after) / 0.0157
+        worst_e = max(worst_e, float((np.abs(e_mixed - e64) / np.maximum(np.abs(e64), 1.0)).max()))
+        n += sel.size
+    return {"step": k, "poses": n, "max_rel_score_err": worst_s, "max_rel_energy_err": worst_e}
 
 
 def time_clustering(dk, cxs):
@@ -350,42 +387,68 @@ def cpu_reference_placement(cfg, folder, device):
             "bit_identical": bool(np.array_equal(cent, c2) and np.array_equal(poses, p2))}
 
 
-def cpu_reference_rate(cfg, budget_s=12.0, seed=0):
+def product_library_mapped() -> bool:
+    """Whether this process has the product library (libsparkle_b200.so) mapped."""
+    try:
+        with open("/proc/self/maps") as f:
+            return "libsparkle_b200.so" in f.read()
+    except OSError:
+        return False
+
+
+def cpu_reference_rate(cfg, budget_s=12.0, seed=0, clean=False):
     """The reference's own CPU scoring path (oracle/_ref: its compiled cdfire_calculate_dfire,
-    rotate and GSO helpers, OpenMP over swarms) on a bounded swarm sample; falls back to the
-    oracle's C restatement when the reference harness was not built."""
+    rotate and GSO helpers, OpenMP over swarms) on a bounded sample of the workload: the first
+    min(S, cores) swarms of every complex (one swarm per host thread, as the reference runs them),
+    all sampled complexes stepped together from the start until the time budget is spent (at
+    least one step).  Each complex's poses and time are scaled by S / sampled swarms, so the rate
+    is that of the workload's own mix of complexes.  Falls back to the oracle's C restatement when
+    the reference harness was not built.  Inputs come from the oracle's restatement of the
+    synthetic generator (bit-identical to the product's), so this leg never loads the product
+    library; with clean=True that is checked before timing."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import sparkledock_b200 as sd
-    from oracle_bind import OracleState, OracleSystem, oracle_step, ref, ref_available, ref_step
+    from oracle_bind import (OracleState, OracleSynthComplex, OracleSystem, oracle_draws, oracle_step, oracle_tables,
+                             ref, ref_available, ref_step)
     cores = os.cpu_count() or 1
-    nr, nl, S = cfg["complexes"][0]
-    sample_s = max(1, min(S, 2 * cores))
-    cx = sd.SyntheticComplex(nr, nl, sample_s, G, 10, 10, seed=100)
-    tables = sd.synthetic_tables(3)
-    osys = OracleSystem(cx, tables, cr_math=0)
-    st = OracleState(sample_s, G, cx.pose_len, cx.poses)
-    U = sd.gso_draws(seed, sample_s, 100, G)
+    cs = cfg["complexes"]
     kind = "reference" if ref_available() else "port"
     if kind == "reference":
         ref()
-    scored = 0
-    t0 = time.perf_counter()
+    tables = oracle_tables(3)
+    samples = [min(S, cores) for _, _, S in cs]
+    systems = []
+    for i, ((a, b, S), k) in enumerate(zip(cs, samples)):
+        cx = OracleSynthComplex(a, b, k, G, 10, 10, seed=100 + i)
+        systems.append((OracleSystem(cx, tables, cr_math=0), OracleState(k, G, cx.pose_len, cx.poses),
+                        oracle_draws(seed + i, k, 100, G)))
+    if clean and product_library_mapped():
+        raise RuntimeError("the reference arm has the product library mapped")
+    scored = [0] * len(cs)
+    secs = [0.0] * len(cs)
     steps = 0
+    t0 = time.perf_counter()
     while steps < 100:
-        before = st.moved.copy(), st.step.copy()
-        if kind == "reference":
-            scored += ref_step(osys, st, U[:, steps, :], cores)
-        else:
-            oracle_step(osys, st, U[:, steps, :], nthreads=cores)
-            scored += int(((before[0] == 1) | (before[1] == 0)).sum())
+        for i, (osys, st, U) in enumerate(systems):
+            t1 = time.perf_counter()
+            if kind == "reference":
+                scored[i] += ref_step(osys, st, U[:, steps, :], cores)
+            else:
+                before = st.moved.copy(), st.step.copy()
+                oracle_step(osys, st, U[:, steps, :], nthreads=cores)
+                scored[i] += int(((before[0] == 1) | (before[1] == 0)).sum())
+            secs[i] += time.perf_counter() - t1
         steps += 1
         if time.perf_counter() - t0 > budget_s:
             break
     dt = time.perf_counter() - t0
-    return {"value": scored / dt, "unit": "scored poses/s", "cores": cores, "kind": kind,
-            "sample": f"{sample_s} of {S} swarms x {G} glowworms, {steps} GSO steps from the start "
-                      f"({scored} poses rescored in {dt:.1f} s, wall clock, OpenMP over swarms)",
-            "steps_per_s_sample": steps / dt}
+    w = [S / k for (_, _, S), k in zip(cs, samples)]
+    value = sum(wi * n for wi, n in zip(w, scored)) / sum(wi * t for wi, t in zip(w, secs))
+    sample = ", ".join(f"{k}/{S}" for k, (_, _, S) in zip(samples, cs))
+    return {"value": value, "unit": "scored poses/s", "cores": cores, "kind": kind,
+            "sample": f"swarms {sample} (of each complex) x {G} glowworms, {steps} GSO steps from the start "
+                      f"({sum(scored)} poses rescored in {dt:.1f} s wall clock, OpenMP over swarms; each "
+                      f"complex's poses and time scaled to its full swarm count)",
+            "steps_per_s_sample": steps / dt, "product_library_mapped": product_library_mapped()}
 
 
 def rank_env():
@@ -404,87 +467,15 @@ def reduce_max_sum(dist, t_ms, scored, device):
     return float(t.item()), int(s.item())
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=97)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c1", choices=sorted(CONFIGS))
-    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison runs")
-    ap.add_argument("--cpu-budget", type=float, default=12.0)
-    ap.add_argument("--swarms", type=int, default=0, help="override the swarm count (profiling of a smaller case)")
-    ap.add_argument("--precision", default="", choices=["", "mixed", "fp64", "fp64_ref"])
-    ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--per-step", action="store_true", help="record scored poses and time of every timed step")
-    args = ap.parse_args()
-    cfg = dict(CONFIGS[args.config])
-    if args.swarms:
-        cfg["complexes"] = [(nr, nl, min(s, args.swarms)) for nr, nl, s in cfg["complexes"]]
-        cfg["workload"] += f" (swarms capped at {args.swarms})"
-    if args.precision and args.precision != cfg.get("precision"):
-        cfg["precision"] = args.precision
-        cfg["workload"] = cfg["workload"].replace("mixed precision", args.precision + " precision")
-    rank, world, local = rank_env()
-    config = {"workload": cfg["workload"], "complexes": [list(c) for c in cfg["complexes"]], "glowworms": G,
-              "anm_modes": [10, 10], "gso_steps": args.warmup + args.steps, "scoring": "dfire",
-              "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{args.gpus}"}
-
-    if args.config == "c4":
-        if rank == 0:
-            import torch
-            torch.cuda.set_device(0)
-            res = run_c4(cfg, 0, args.warmup + args.steps)
-            print(json.dumps({"metric": "pyDock-style adjoint poses/s (energy + 26-dim gradient, host buffers)",
-                              "value": res["fp32"]["poses_per_s"], "unit": "poses/s", "n_gpus": 1,
-                              "higher_is_better": True, "data": "synthetic", "config": config, **res}))
-        return
-
-    if args.impl == "reference":
-        if rank != 0:
-            return
-        cb = cpu_reference_rate(cfg, args.cpu_budget)
-        line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "scored poses/s",
-                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
-                "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
-                "e2e": {"value": cb["value"], "unit": "scored poses/s", "h2d_bytes_per_step": 0,
-                        "d2h_bytes_per_step": 0}}
-        print(json.dumps(line))
-        return
-
-    import torch
-    dist = None
-    if world > 1:
-        import torch.distributed as dist_mod
-        dist_mod.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-        dist = dist_mod
-    device = local if world > 1 else 0
-    torch.cuda.set_device(device)
-    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize(device)
-
-    barrier()
-    with Clocks(device) as clk:
-        run = run_gpu(cfg, cfg["precision"], args.steps, args.warmup, device, flush, per_step=args.per_step)
-    barrier()
+def measure(cfg, name, args, device, flush, dist, energy_every=0):
+    """The workload of one configuration: the timed mixed (or the configuration's precision)
+    steps, then the plain FP64 kernels over the same trajectory for the mixed-vs-FP64 ratio."""
+    run = run_gpu(cfg, cfg["precision"], args.steps, args.warmup, device, flush, per_step=args.per_step,
+                  energy_every=energy_every)
     t_ms, scored = reduce_max_sum(dist, sum(run["ms"]), run["scored"], device)
     _, pairs_all = reduce_max_sum(dist, 0.0, run["pairs"], device)  # every rank takes part
     value = scored / (t_ms / 1e3)
-    stats = run["stats"]
-    pairs_timed_rank = run["pairs"]
-    tuning = run["tuning"]
-    spot = fp64_spot_check(run["ctx"], run["cxs"]) if cfg["precision"] == "mixed" else None
-    clustering = time_clustering(run["ctx"], run["cxs"])
-    run["ctx"].close()
-    setup_dir = tempfile.mkdtemp(prefix="sd_setup_") if rank == 0 else None
-    setup = time_setup(cfg, setup_dir, device) if rank == 0 else None
-
+    out = {"run": run, "t_ms": t_ms, "scored": scored, "pairs_all": pairs_all, "value": value}
     extra = {}
     if not args.no_fp64 and cfg["precision"] == "mixed":
         # the FP64 runs take the same trajectory; on the large configurations they are bounded to
@@ -508,13 +499,157 @@ def main():
             # per in-cutoff pair at the mixed run's pairs per pose on the large receptor) over the
             # nominal FP64 vector pipe: 148 SMs x 64 lanes x 2 at the measured max SM clock
             fp64_peak = 148 * 64 * 2 * (measured_peaks()[0].get("sm_max_mhz", 1965.0) * 1e6) / 1e12
-            per_pose = (8.0 * brute_pairs_per_pose(cfg) if args.config != "c3" else
-                        8.0 * pairs_all / max(1, scored))
+            per_pose = (8.0 * brute_pairs_per_pose(cfg) if name != "c3" else 8.0 * pairs_all / max(1, scored))
             ach = per_pose * sc / (tm / 1e3) / 1e12
             extra[pname]["roofline"] = {"bound": "fp64", "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
                                         "frac": ach / fp64_peak,
                                         "peak_source": "nominal FP64 vector pipe (148 SMs x 64 lanes x 2) at the "
                                                        "measured max SM clock"}
+    out["mixed_vs_fp64"] = extra
+    errs = run["energy_err"]
+    if errs:
+        out["per_step_energy_error"] = {
+            "steps_checked": len(errs), "every": energy_every,
+            "max_rel_energy_err": max(e["max_rel_energy_err"] for e in errs),
+            "max_rel_score_err": max(e["max_rel_score_err"] for e in errs),
+            "poses_checked": sum(e["poses"] for e in errs), "tolerance": 1e-5,
+            "reference": "plain FP64 kernel (bit-identical to the FP64 oracle) on the poses each step rescored",
+            "per_step_max_rel_energy_err": [e["max_rel_energy_err"] for e in errs]}
+    return out
+
+
+def roofline_of(cfg, name, m, args, peaks, peak_src):
+    """Roofline of the timed steps: the scorer's work over the FP32 vector pipe (the scorer is
+    neither HBM- nor tensor-shaped: its tables stay in L2 and its distance contraction has K = 3).
+    Primary: 8 flops per receptor-ligand pair inside the cutoff (the work the culled kernel does,
+    counted by the kernel); beside it the brute-force-equivalent 8 Nr Nl flops per scored pose
+    (the reference's formulation of the DFIRE sum).  Time: the timed GSO steps (scorer ~99 %)."""
+    stats = m["run"]["stats"]
+    t_s = m["t_ms"] / 1e3
+    fp32_peak = 148 * 128 * 2 * (peaks.get("sm_max_mhz", 1965.0) * 1e6) / 1e12
+    cut_tflops = 8.0 * m["pairs_all"] / t_s / 1e12
+    brute = 8.0 * brute_pairs_per_pose(cfg) * m["scored"] / t_s / 1e12
+    return {"bound": "fp32", "achieved": cut_tflops, "peak": fp32_peak, "unit": "TFLOP/s",
+            "frac": cut_tflops / fp32_peak,
+            "work": "8 flops per receptor-ligand pair inside the 15 A cutoff (counted by the kernel)",
+            "pairs_per_s": m["pairs_all"] / t_s,
+            "table_bytes_per_s": 8.0 * m["pairs_all"] / t_s,
+            "traffic": DRAM_BYTES_PER_LAUNCH + DRAM_BYTES_PER_SCORED_POSE * m["scored"] / args.steps,
+            "traffic_unit": "bytes per launch (DRAM, ncu: fixed + per rescored pose)",
+            "peak_source": "nominal FP32 vector pipe (148 SMs x 128 lanes x 2) at the measured "
+                           f"max SM clock {peaks.get('sm_max_mhz', 1965.0):.0f} MHz "
+                           f"({peak_src} peaks file has no FP32 vector figure)",
+            "hbm_frac": (DRAM_BYTES_PER_LAUNCH * args.steps / t_s +
+                         DRAM_BYTES_PER_SCORED_POSE * m["value"]) / 1e9 / peaks.get("hbm_gbs", 6650.0),
+            "brute_force_equivalent": {"tflops": brute, "frac": brute / fp32_peak,
+                                       "work": "8 Nr Nl flops per scored pose"},
+            "per_scored_pose": {"pairs_in_cutoff": stats["pairs_in_cutoff"] / max(1, stats["scored_poses"]),
+                                "pairs_evaluated": stats["pairs_evaluated"] / max(1, stats["scored_poses"]),
+                                "pairs_brute_force": brute_pairs_per_pose(cfg)}}
+
+
+def config_of(cfg, args):
+    return {"workload": cfg["workload"], "complexes": [list(c) for c in cfg["complexes"]], "glowworms": G,
+            "anm_modes": [10, 10], "gso_steps": args.warmup + args.steps, "scoring": "dfire",
+            "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{args.gpus}"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=97)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison runs")
+    ap.add_argument("--no-c1", action="store_true", help="skip the single-complex leg of the batched workload")
+    ap.add_argument("--cpu-budget", type=float, default=12.0)
+    ap.add_argument("--swarms", type=int, default=0, help="override the swarm count (profiling of a smaller case)")
+    ap.add_argument("--precision", default="", choices=["", "mixed", "fp64", "fp64_ref"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-setup", action="store_true", help="skip the setup-stage and clustering timings")
+    ap.add_argument("--per-step", action="store_true", help="record scored poses and time of every timed step")
+    args = ap.parse_args()
+    cfg = dict(CONFIGS[args.config])
+    if args.swarms:
+        cfg["complexes"] = [(nr, nl, min(s, args.swarms)) for nr, nl, s in cfg["complexes"]]
+        cfg["workload"] += f" (swarms capped at {args.swarms})"
+    if args.precision and args.precision != cfg.get("precision"):
+        cfg["precision"] = args.precision
+        cfg["workload"] = cfg["workload"].replace("mixed precision", args.precision + " precision")
+    rank, world, local = rank_env()
+    config = config_of(cfg, args)
+
+    if args.config == "c4":
+        if rank == 0:
+            import torch
+            torch.cuda.set_device(0)
+            res = run_c4(cfg, 0, args.warmup + args.steps)
+            print(json.dumps({"metric": "pyDock-style adjoint poses/s (energy + 26-dim gradient, host buffers)",
+                              "value": res["fp32"]["poses_per_s"], "unit": "poses/s", "n_gpus": 1,
+                              "higher_is_better": True, "data": "synthetic", "config": config, **res}))
+        return
+
+    if args.impl == "reference":
+        # the reference's own CPU path on rank 0 only; inputs from the oracle, the product library
+        # is never loaded in this process (checked before timing)
+        if rank != 0:
+            return
+        cb = cpu_reference_rate(cfg, args.cpu_budget, clean=True)
+        line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "scored poses/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+                "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": cb["value"], "unit": "scored poses/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0},
+                "product_library_mapped": cb["product_library_mapped"]}
+        print(json.dumps(line))
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        dist_mod.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        dist = dist_mod
+    device = local if world > 1 else 0
+    torch.cuda.set_device(device)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(device)
+
+    # the configuration's own steps: energies checked every 10th step on the batched workload (its
+    # state is 138 MB), every step otherwise; the check runs between steps, outside the events
+    energy_every = 0 if cfg["precision"] != "mixed" else (10 if len(cfg["complexes"]) > 1 else 1)
+    barrier()
+    with Clocks(device) as clk:
+        m = measure(cfg, args.config, args, device, flush, dist, energy_every=energy_every)
+    barrier()
+    run = m["run"]
+    stats = run["stats"]
+    spot = fp64_spot_check(run["ctx"], run["cxs"]) if cfg["precision"] == "mixed" else None
+    clustering = None if args.no_setup else time_clustering(run["ctx"], run["cxs"])
+    run["ctx"].close()
+    setup_dir = tempfile.mkdtemp(prefix="sd_setup_") if rank == 0 else None
+    setup = time_setup(cfg, setup_dir, device) if rank == 0 and not args.no_setup else None
+
+    # the single-complex workload beside the batched one: its own rate and mixed-vs-FP64 ratio
+    c1 = None
+    if args.config == "c2" and not args.no_c1 and not args.swarms and not args.precision:
+        cfg1 = dict(CONFIGS["c1"])
+        with Clocks(device) as clk1:
+            m1 = measure(cfg1, "c1", args, device, flush, dist, energy_every=1)
+        m1["run"]["ctx"].close()
+        c1 = {"workload": cfg1["workload"], "complexes": [list(c) for c in cfg1["complexes"]],
+              "value": m1["value"], "unit": "scored poses/s", "ms_per_step": m1["t_ms"] / args.steps,
+              "steps_per_s": args.steps / (m1["t_ms"] / 1e3), "mixed_vs_fp64": m1["mixed_vs_fp64"],
+              "per_step_energy_error": m1.get("per_step_energy_error"), "clocks": clk1.summary(),
+              "autotuner": m1["run"]["tuning"]}
+
     if args.no_e2e:
         e2e = {"ms": float("nan"), "wall_s": None, "scored": 0, "h2d": 0, "d2h": 0}
     else:
@@ -527,12 +662,9 @@ def main():
         return
     peaks, peak_src = measured_peaks()
     clocks = clk.summary()
-    # algorithmic work: 8 flops per receptor-ligand pair inside the 15 A cutoff (distance:
-    # 3 sub + 3 mul + 2 add); P_cut counted by the kernel
-    pairs = stats.get("pairs_in_cutoff", None)
-    fp32_peak = 148 * 128 * 2 * (peaks.get("sm_max_mhz", 1965.0) * 1e6) / 1e12
+    t_ms = m["t_ms"]
     line = {
-        "metric": METRIC, "value": value, "unit": "scored poses/s", "n_gpus": world, "steps": args.steps,
+        "metric": METRIC, "value": m["value"], "unit": "scored poses/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "steps_per_s": args.steps / (t_ms / 1e3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 pairs, f64 GSO",
         "data": "synthetic (seeded globules, N(0,1) DFIRE table)", "config": config,
@@ -540,53 +672,30 @@ def main():
         "e2e": {"value": es / (et / 1e3), "unit": "scored poses/s", "h2d_bytes_per_step": e2e["h2d"],
                 "d2h_bytes_per_step": e2e["d2h"], "wall_s": e2e["wall_s"]},
         "clocks": clocks,
-        "mixed_vs_fp64": extra,
-        "autotuner": tuning,
+        "mixed_vs_fp64": m["mixed_vs_fp64"],
+        "per_step_energy_error": m.get("per_step_energy_error"),
+        "autotuner": run["tuning"],
         "fp64_spot_check": spot,
+        "c1": c1,
         "final_clustering": clustering,
         "setup": setup,
         **({"per_step": {"scored_poses": run["per_step"], "ms": run["ms"]}} if args.per_step else {}),
         "edge_counts": {k: stats[k] for k in ("pairs_fallback", "edge_d2_zero", "edge_d2_cutoff", "edge_u_zero",
                                               "edge_shortfall")},
-        "per_scored_pose": {"pairs_in_cutoff": stats["pairs_in_cutoff"] / max(1, stats["scored_poses"]),
-                            "pairs_evaluated": stats["pairs_evaluated"] / max(1, stats["scored_poses"]),
-                            "pairs_brute_force": brute_pairs_per_pose(cfg)},
     }
-    if pairs:
-        # algorithmic work per scored pose: W = 8 Nr Nl flops (3 sub + 3 mul + 2 add per pair, the
-        # reference's brute-force formulation of the DFIRE sum), or W = 8 P_cut (pairs inside the
-        # cutoff, counted by the kernel) for the large-receptor workload, whose reference runs a
-        # cutoff grid; bound: the FP32 vector pipe (the scorer is neither HBM- nor tensor-shaped:
-        # its tables stay in L2 and its distance contraction has K = 3).  Time: the timed GSO
-        # steps, of which the scorer is 99.5 %.
-        brute = args.config != "c3"
-        w_pose = 8.0 * line["per_scored_pose"]["pairs_brute_force"] if brute else None
-        achieved = (w_pose * scored if brute else 8.0 * pairs_all) / (t_ms / 1e3) / 1e12
-        cut_tflops = 8.0 * pairs_all / (t_ms / 1e3) / 1e12
-        line["roofline"] = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                            "frac": achieved / fp32_peak,
-                            "work": ("8 Nr Nl flops per scored pose" if brute else
-                                     "8 flops per receptor-ligand pair inside the cutoff"),
-                            "traffic": DRAM_BYTES_PER_LAUNCH + DRAM_BYTES_PER_SCORED_POSE * scored / args.steps,
-                            "traffic_unit": "bytes per launch (DRAM, ncu: fixed + per rescored pose)",
-                            "peak_source": "nominal FP32 vector pipe (148 SMs x 128 lanes x 2) at the measured "
-                                           f"max SM clock {peaks.get('sm_max_mhz', 1965.0):.0f} MHz "
-                                           f"({peak_src} peaks file has no FP32 vector figure)",
-                            "hbm_frac": (DRAM_BYTES_PER_LAUNCH * args.steps / (t_ms / 1e3) +
-                                         DRAM_BYTES_PER_SCORED_POSE * value) / 1e9 / peaks.get("hbm_gbs", 6650.0),
-                            "in_cutoff_pairs": {"tflops": cut_tflops, "frac": cut_tflops / fp32_peak,
-                                                "pairs_per_s": pairs_all / (t_ms / 1e3),
-                                                "table_bytes_per_s": 8.0 * pairs_all / (t_ms / 1e3)}}
+    if stats.get("pairs_in_cutoff"):
+        line["roofline"] = roofline_of(cfg, args.config, m, args, peaks, peak_src)
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
             line["cpu_baseline"] = {k: v for k, v in cpu_reference_rate(cfg, args.cpu_budget).items()
                                     if k in ("value", "unit", "cores", "kind", "sample")}
         except Exception as e:  # the baseline is reported, never required
             line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
-        try:
-            setup["reference_cpu"] = cpu_reference_placement(cfg, setup_dir, device)
-        except Exception as e:
-            setup["reference_cpu"] = {"value": None, "error": str(e)[:200]}
+        if setup is not None:
+            try:
+                setup["reference_cpu"] = cpu_reference_placement(cfg, setup_dir, device)
+            except Exception as e:
+                setup["reference_cpu"] = {"value": None, "error": str(e)[:200]}
     shutil.rmtree(setup_dir, ignore_errors=True)
     print(json.dumps(line))
     if dist is not None:

@@ -98,6 +98,28 @@ double or_acos_cr(double x);
 /* slerp of the reference (prepare_gso_tasks.cc:1370-1421) with cr or libm math */
 void or_slerp(double* self, double* other, double step, int cr_math);
 
+/* Seeded synthetic complexes and tables, restating the product's generator (or_synth.c):
+ * caller-allocated arrays of the given sizes. */
+typedef struct {
+  double* rec_xyz;     /* [nr][3] */
+  double* lig_xyz;     /* [nl][3] */
+  double* rec_modes;   /* [nmr][nr][3] */
+  double* lig_modes;   /* [nml][nl][3] */
+  double* rec_charge;  /* [nr] */
+  double* lig_charge;  /* [nl] */
+  double* poses;       /* [S][G][7+nmr+nml] */
+  int* rec_mask;
+  int* lig_mask;
+  int* rec_type;
+  int* lig_type;
+  int* rec_lj;
+  int* lig_lj;
+  double lig_ref[3];   /* Khachiyan centre of the ligand, tolerance 0.01 */
+} or_synth_out;
+void or_synth_generate(int nr, int nl, int S, int G, int nmr, int nml, unsigned long long seed, or_synth_out* o);
+void or_synth_tables(unsigned long long seed, double* dfire, double* eps, double* sigma);
+void or_mvee_center(const double* p, int n, double tol, double* center);
+
 /* Exact key thresholds: smallest double x with (int)(sqrt(x)*2.0-1.0) >= m, m = 1..29 */
 void or_key_thresholds(double* t30);
 

@@ -41,6 +41,13 @@ class OrCounts(C.Structure):
     _fields_ = [(n, C.c_longlong) for n in ("scored", "d2_zero", "d2_cutoff", "u_zero", "shortfall")]
 
 
+class OrSynthOut(C.Structure):
+    _fields_ = [(n, _dp) for n in ("rec_xyz", "lig_xyz", "rec_modes", "lig_modes", "rec_charge", "lig_charge",
+                                   "poses")] + \
+               [(n, _ip) for n in ("rec_mask", "lig_mask", "rec_type", "lig_type", "rec_lj", "lig_lj")] + \
+               [("lig_ref", C.c_double * 3)]
+
+
 def _d(a):
     return a.ctypes.data_as(_dp)
 
@@ -74,8 +81,57 @@ def oracle():
         L.or_pydock_energy.restype = C.c_double
         L.or_pydock_energy.argtypes = [C.POINTER(OrSystem), _dp]
         L.or_pydock_grad.argtypes = [C.POINTER(OrSystem), _dp, _dp]
+        L.or_synth_generate.argtypes = [C.c_int] * 6 + [C.c_ulonglong, C.POINTER(OrSynthOut)]
+        L.or_synth_tables.argtypes = [C.c_ulonglong, _dp, _dp, _dp]
+        L.or_mvee_center.argtypes = [_dp, C.c_int, C.c_double, _dp]
         _oracle = L
     return _oracle
+
+
+class OracleSynthComplex:
+    """A seeded synthetic complex built by the oracle's restatement of the product's generator
+    (oracle/or_synth.c), bit-identical to sparkledock_b200.SyntheticComplex with the same
+    arguments, without loading the product library."""
+
+    def __init__(self, n_rec, n_lig, n_swarms, n_glowworms=200, n_modes_rec=10, n_modes_lig=10, seed=1):
+        self.n_rec, self.n_lig = n_rec, n_lig
+        self.n_swarms, self.n_glowworms = n_swarms, n_glowworms
+        self.n_modes_rec, self.n_modes_lig = n_modes_rec, n_modes_lig
+        self.pose_len = 7 + n_modes_rec + n_modes_lig
+        self.rec_xyz = np.zeros((n_rec, 3))
+        self.lig_xyz = np.zeros((n_lig, 3))
+        self.rec_modes = np.zeros((n_modes_rec, n_rec, 3))
+        self.lig_modes = np.zeros((n_modes_lig, n_lig, 3))
+        self.rec_charge = np.zeros(n_rec)
+        self.lig_charge = np.zeros(n_lig)
+        self.poses = np.zeros((n_swarms, n_glowworms, self.pose_len))
+        self.rec_mask, self.lig_mask = np.zeros(n_rec, np.int32), np.zeros(n_lig, np.int32)
+        self.rec_type, self.lig_type = np.zeros(n_rec, np.int32), np.zeros(n_lig, np.int32)
+        self.rec_lj, self.lig_lj = np.zeros(n_rec, np.int32), np.zeros(n_lig, np.int32)
+        o = OrSynthOut()
+        for f in ("rec_xyz", "lig_xyz", "rec_modes", "lig_modes", "rec_charge", "lig_charge", "poses"):
+            setattr(o, f, _d(getattr(self, f)))
+        for f, a in (("rec_mask", "rec_mask"), ("lig_mask", "lig_mask"), ("rec_type", "rec_type"),
+                     ("lig_type", "lig_type"), ("rec_lj", "rec_lj"), ("lig_lj", "lig_lj")):
+            setattr(o, f, _i(getattr(self, a)))
+        oracle().or_synth_generate(n_rec, n_lig, n_swarms, n_glowworms, n_modes_rec, n_modes_lig, seed, C.byref(o))
+        self.lig_ref = np.array(list(o.lig_ref), np.float64)
+
+
+def oracle_tables(seed: int = 2024):
+    """The seeded N(0,1) DFIRE table and LJ table (oracle restatement of the product's)."""
+    t = np.empty(168 * 168 * 20)
+    e = np.empty(20)
+    s = np.empty(20)
+    oracle().or_synth_tables(seed, _d(t), _d(e), _d(s))
+    return t, e, s
+
+
+def oracle_draws(seed: int, n_swarms: int, n_steps: int, n_glowworms: int) -> np.ndarray:
+    """The reference's draws u[s][t][g] (mt19937 + uniform_real_distribution, oracle restatement)."""
+    out = np.empty((n_swarms, n_steps, n_glowworms))
+    oracle().or_gso_draws(seed, n_swarms, n_steps, n_glowworms, _d(out))
+    return out
 
 
 def ref_available() -> bool:

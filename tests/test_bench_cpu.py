@@ -22,6 +22,9 @@ def test_reference_arm_json_line():
     assert d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0
     assert d["cpu_baseline"]["kind"] in ("reference", "port") and d["cpu_baseline"]["cores"] >= 1
     assert d["config"]["workload"]
+    # the reference arm builds its inputs from the oracle and never loads the product library
+    assert d["product_library_mapped"] is False
+    assert len(d["config"]["complexes"]) == 8  # the default workload: the batched eight complexes
 
 
 def test_work_per_pose_weighted_by_swarms():

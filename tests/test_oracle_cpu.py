@@ -224,3 +224,22 @@ def test_pydock_oracle_gradient_matches_finite_differences(tables):
         f = fd_grad(osys, pose, ng)
         scale = max(np.abs(g).max(), 1.0)
         assert np.abs(g - f).max() / scale < 1e-6, (g, f)
+
+
+def test_oracle_synthetic_generator_equals_product():
+    """The oracle's restatement of the seeded synthetic generator (used by the benchmark's reference
+    arm, which must not load the product library) writes exactly the product's arrays, tables and
+    draws, for several sizes, mode counts and seeds."""
+    import sparkledock_b200 as sd
+    from oracle_bind import OracleSynthComplex, oracle_draws, oracle_tables
+    fields = ("rec_xyz", "lig_xyz", "rec_modes", "lig_modes", "rec_charge", "lig_charge", "poses", "rec_mask",
+              "lig_mask", "rec_type", "lig_type", "rec_lj", "lig_lj", "lig_ref")
+    for nr, nl, S, G, mr, ml, seed in ((757, 481, 3, 20, 10, 10, 100), (2039, 1440, 2, 7, 10, 10, 101),
+                                       (300, 64, 2, 5, 0, 3, 9), (17, 9, 1, 3, 2, 0, 0)):
+        a = OracleSynthComplex(nr, nl, S, G, mr, ml, seed=seed)
+        b = sd.SyntheticComplex(nr, nl, S, G, mr, ml, seed=seed)
+        for f in fields:
+            assert np.array_equal(getattr(a, f), getattr(b, f)), (nr, nl, f)
+    for x, y in zip(oracle_tables(3), sd.synthetic_tables(3)):
+        assert np.array_equal(x, y)
+    assert np.array_equal(oracle_draws(7, 3, 4, 11), sd.gso_draws(7, 3, 4, 11))
