@@ -123,7 +123,6 @@ typedef struct {
   long long timeouts;           /* bounded device waits that gave up */
   long long pairs_in_cutoff;    /* receptor-ligand pairs with d^2 <= 225 met while rescoring (GSO steps) */
   long long pairs_evaluated;    /* pair distances computed after culling (GSO steps) */
-  long long guard_errors;       /* reserved, always 0: the scorers' indices are in range by construction */
 } sd_stats;
 
 typedef struct sd_ctx sd_ctx;
@@ -289,8 +288,13 @@ int sd_score_poses(sd_ctx* ctx, int complex_idx, const double* poses, int n, int
  * array that every GPU loading this library holds until exit; all calls on a device share it
  * and each call rewrites it first, so calls whose GPU work overlaps (other streams or contexts
  * on the same device) race and must be ordered by the caller.  Runs on the context stream,
- * asynchronously unless sync != 0.  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress); make that first call before any stream capture. */
+ * asynchronously unless sync != 0.  sync must be 0 while the stream is being captured (a
+ * synchronisation would invalidate the capture; SD_ERR_ARG).  Poses must be finite: with
+ * sync != 0 the call also counts non-finite pose values on the device and returns
+ * SD_ERR_NUMERIC if there are any (the outputs of such a call are not meaningful); with sync == 0
+ * nothing is checked.  These calls do not add to the counters of sd_get_stats.  The first call on
+ * a device (and the first after a cudaDeviceReset) looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture. */
 int sd_score_poses_noalloc(sd_ctx* ctx, int complex_idx, const double* d_poses, int n, int precision,
                            double* d_score, double* d_energy, double* d_ref, int sync);
 
@@ -338,6 +342,11 @@ int sd_checkpoint_info(const char* path, int* n_swarms, int* n_glowworms, int* p
  * poses [n][pose_len] in/out (host); energy_before / energy_after [n] FP64 energies (nullable). */
 int sd_refine_poses(sd_ctx* ctx, int complex_idx, double* poses, int n, int iters, double step, int precision,
                     double* energy_before, double* energy_after);
+
+/* Diagnostics: the correctly rounded acos (fn 0) and sin (fn 1) that the GSO update's slerp
+ * (prepare_gso_tasks.cc:1370-1421) uses, evaluated by a device kernel on n host values x into
+ * out (parity checking of the device arithmetic against a host restatement). */
+int sd_crmath_eval(int device, int fn, const double* x, long long n, double* out);
 
 /* ---- synthetic complexes (seeded), for tests and benchmarks ---- */
 typedef struct {

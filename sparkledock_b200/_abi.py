@@ -62,7 +62,7 @@ class SwarmState(C.Structure):
 class Stats(C.Structure):
     _fields_ = [(n, C.c_longlong) for n in (
         "scored_poses", "steps", "pairs_fallback", "edge_d2_zero", "edge_d2_cutoff",
-        "edge_u_zero", "edge_shortfall", "timeouts", "pairs_in_cutoff", "pairs_evaluated", "guard_errors")]
+        "edge_u_zero", "edge_shortfall", "timeouts", "pairs_in_cutoff", "pairs_evaluated")]
 
 
 class SynthSpec(C.Structure):
@@ -123,6 +123,7 @@ SIGNATURES = {
     "sd_synth_generate": (C.c_int, [C.POINTER(SynthSpec), C.c_void_p, C.POINTER(ComplexDesc),
                                     C.POINTER(_dp)]),
     "sd_synth_tables": (C.c_int, [C.c_ulonglong, _dp, _dp, _dp]),
+    "sd_crmath_eval": (C.c_int, [C.c_int, C.c_int, _dp, C.c_longlong, _dp]),
 }
 
 _lib = None

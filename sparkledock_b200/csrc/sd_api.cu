@@ -962,7 +962,6 @@ int sd_get_stats(sd_ctx* c, sd_stats* out) {
   out->timeouts = (long long)(a.stats[ST_TIMEOUT] + b.stats[ST_TIMEOUT]);
   out->pairs_in_cutoff = (long long)a.stats[ST_PAIRS];
   out->pairs_evaluated = (long long)a.stats[ST_EVALS];
-  out->guard_errors = 0;  // reserved: the mixed kernel's ring indices are masked into range
   return SD_OK;
 }
 

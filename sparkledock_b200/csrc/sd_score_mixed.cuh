@@ -12,17 +12,16 @@
 //    rejects ligand chunks by bounding spheres and ligand atoms by ballot, and stages the
 //    surviving candidates 32 at a time into one of two per-warp batch buffers, in the bit order
 //    of the stage-1 mask (candidate 2i at position i, 2i+1 at position 16+i);
-//  * stage 1 (kH16) tests a pair with the dot-product form of the distance in packed FP16,
-//    three HFMA2 per two candidates: s = r.l - |l|^2/2 >= (|r|^2 - thr)/2, on coordinates
-//    centred on the tile centre.  thr is set per tile from a proven bound on the FP16 error
-//    (below), so every pair whose FP32 d^2 is within the cutoff passes; tiles or poses whose
-//    magnitudes would make the bound loose pass every candidate, and stage 2 filters exactly.
-//    Without kH16 the test is the FP32 d^2 itself;
+//  * stage 1 tests a pair with the dot-product form of the distance in packed FP16, three
+//    HFMA2 per two candidates: s = r.l - |l|^2/2 >= (|r|^2 - thr)/2, on coordinates centred on
+//    the tile centre.  thr is set per tile from a proven bound on the FP16 error (below), so
+//    every pair whose FP32 d^2 is within the cutoff passes; tiles or poses whose magnitudes
+//    would make the bound loose pass every candidate, and stage 2 filters exactly;
 //  * in-cutoff pairs are appended to a per-warp ring of 16-bit entries (buffer, position,
-//    receptor lane) by a warp scan; stage 2 drains it 32 or 64 entries per round (kDual: two per
-//    lane), reads the candidate and the receptor atom from 4-byte arrays and a float4 (mostly
-//    broadcast reads), recomputes the FP32 d^2 and takes the key from a fast reciprocal square
-//    root.  The key's edges ((k+1)/2)^2 and ((k+2)/2)^2 (the upper one stopped at the cutoff) are
+//    receptor lane) by a warp scan; stage 2 drains it 64 entries per round (two per lane), reads
+//    the candidate and the receptor atom from 4-byte arrays and a float4 (mostly broadcast
+//    reads), recomputes the FP32 d^2 and takes the key from a fast reciprocal square root.  The
+//    key's edges ((k+1)/2)^2 and ((k+2)/2)^2 (the upper one stopped at the cutoff) are
 //    compared with d^2 - edge computed with one rounding against the FP32 error bound B, so a
 //    pair that is not near an edge has its FP64 bin proven; near pairs are recomputed from the
 //    exact FP64 transform (counted as fallbacks);
@@ -31,8 +30,12 @@
 //    so no bin lookup is needed; a rejected or padding pair gathers a zero past the table instead
 //    of branching, and each round's gathers (through L2 only) are added by the next round, so
 //    they are in flight while the next round is evaluated.  Each lane sums its values in FP64
-//    (Kahan sums of an FP32-rounded table were measured to miss 1e-5 at 60k pairs per pose);
-//    warp shuffles and a block reduction in FP64 finish the pose.
+//    (Kahan sums of an FP32-rounded table were measured to miss 1e-5 at 60k pairs per pose).
+//  * Fixed summation order: a tile's lane sums are reduced by warp shuffles when the tile is
+//    done and stored in a per-pose shared slot of that tile; at the pose end warp 0 adds the
+//    slots in a fixed order.  What happens inside a tile depends only on the pose and the tile,
+//    never on which warp took it or when, and no compiled variant changes it, so a pose's energy
+//    is the same bits in every run, every variant and every entry point.
 //
 // FP16 bound (u = 2^-11, R >= |r - c| for the tile's atoms, Lb >= |l - c| for its candidates,
 // w = |l - c|^2 / 2):  |s_fp16 - (r.l - w)| <= u (2.001 R Lb + w) + 3u (1.002 R Lb + 1.001 w)
@@ -78,11 +81,11 @@ struct __align__(16) RingBufs {
 
 }  // namespace
 
-// kH16: packed-FP16 stage-1 test (else FP32).  kDual: stage 2 takes 64 ring entries per round,
-// two per lane (else 32, one per lane).
-template <int kWarps, int kMinBlocks, bool kH16, bool kDual>
+// Variants differ only in warps per CTA and resident CTAs per SM: a tile is always processed by
+// one warp in the same way, so they give identical energies.
+template <int kWarps, int kMinBlocks>
 __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_kernel(ScoreLaunch L) {
-  constexpr int kG = kDual ? 64 : 32;  // entries per stage-2 round
+  constexpr int kG = 64;  // entries per stage-2 round, two per lane
   constexpr int kSortMax = 512;        // near tiles ordered largest-first up to this many
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ RingBufs wb[kWarps];
@@ -90,7 +93,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
   __shared__ double sh_q[4], sh_qi[4];
   __shared__ double sh_T[32];
   __shared__ float sh_gc[3];      // ligand centroid, rotated (centred on t)
-  __shared__ double sh_red[kWarps];
+  __shared__ double sh_red[1];
   __shared__ int sh_item, sh_ntile, sh_next;
   __shared__ float sh_bound[4];
   __shared__ float sh_rot[9];
@@ -182,7 +185,8 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
     const double tx = sh_pose[0], ty = sh_pose[1], tz = sh_pose[2];
     const float dR = sh_bound[0], dL = sh_bound[1], B = sh_bound[2];
     const int nls = nlc * SD_TILE, ntiles = C.ntiles;
-    float4* ligS = reinterpret_cast<float4*>(smem);  // [nls] centred on t, col bits
+    double* tsum = reinterpret_cast<double*>(smem);  // [ntiles] FP64 energy of each tile of the pose
+    float4* ligS = reinterpret_cast<float4*>(tsum + ((ntiles + 1) & ~1));  // [nls] centred on t, col bits
     float4* chS = ligS + nls;                        // [nlc] centre + radius
     int* tlist = reinterpret_cast<int*>(chS + nlc);  // [ntiles] tiles within reach
     int* tord = tlist + ntiles;                      // [ntiles] the same, largest first
@@ -196,6 +200,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
       chS[c] = make_float4(X, Y, Z, cc.w + dL);
       cneed[c] = 0;
     }
+    for (int k = tid; k < ntiles; k += blockDim.x) tsum[k] = 0.0;
     const float lig_reach = C.lig_radius + dL;
     for (int k = tid; k < ntiles; k += blockDim.x) {
       const float4 tile = C.r_tile[k];
@@ -290,7 +295,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
       __half2 rx2, ry2, rz2, a2;
       const float R = tile.w + dR + SD_CULL_MARGIN, Lb = reach + 0.01f;
       const bool tight = R <= 40.0f && Lb <= 80.0f;  // warp-uniform
-      if (kH16) {
+      {
         const float u16 = 4.8828125e-4f;
         const float Es = u16 * (5.1f * R * Lb + 2.1f * Lb * Lb);
         const float thr0 = 225.0f + B + 1e-3f + 2.0f * Es;
@@ -352,7 +357,7 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
           W.candf[2][par * 32 + pos] = l4.z;
           W.candf[3][par * 32 + pos] = l4.w;
           W.cslot[par * 32 + pos] = (unsigned short)s;
-          if (kH16) {
+          {
             // unused place: s = -60000, never in range; loose tile: every place passes
             float lx = 0.f, ly = 0.f, lz = 0.f, nw = tight ? -60000.f : 0.f;
             if (lane < nb && tight) {
@@ -377,24 +382,13 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
           __syncwarp();
           // stage 1: bit b of m <=> (this lane's receptor atom, candidate at position b) in range
           unsigned M = 0;
-          if (kH16) {
 #pragma unroll
-            for (int i = 0; i < 16; ++i) {
-              const uint4 qq = *reinterpret_cast<const uint4*>(W.candh[i]);
-              __half2 sv = __hfma2(rx2, *reinterpret_cast<const __half2*>(&qq.x), *reinterpret_cast<const __half2*>(&qq.w));
-              sv = __hfma2(ry2, *reinterpret_cast<const __half2*>(&qq.y), sv);
-              sv = __hfma2(rz2, *reinterpret_cast<const __half2*>(&qq.z), sv);
-              M |= __hge2_mask(sv, a2) & (0x00010001u << i);
-            }
-          } else {
-#pragma unroll
-            for (int b = 0; b < 32; ++b) {
-              const float lx = W.candf[0][par * 32 + b], ly = W.candf[1][par * 32 + b],
-                          lz = W.candf[2][par * 32 + b];
-              const float ex = fx - lx, ey = fy - ly, ez = fz - lz;
-              const float d2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
-              M |= (d2 <= cut2 ? 1u : 0u) << b;
-            }
+          for (int i = 0; i < 16; ++i) {
+            const uint4 qq = *reinterpret_cast<const uint4*>(W.candh[i]);
+            __half2 sv = __hfma2(rx2, *reinterpret_cast<const __half2*>(&qq.x), *reinterpret_cast<const __half2*>(&qq.w));
+            sv = __hfma2(ry2, *reinterpret_cast<const __half2*>(&qq.y), sv);
+            sv = __hfma2(rz2, *reinterpret_cast<const __half2*>(&qq.z), sv);
+            M |= __hge2_mask(sv, a2) & (0x00010001u << i);
           }
           const unsigned lo = (1u << ((nb + 1) >> 1)) - 1u, hi = (1u << (nb >> 1)) - 1u;
           unsigned m = M & (lo | (hi << 16)) & (active ? 0xffffffffu : 0u);
@@ -472,10 +466,8 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
           const int n = min(kG, upto - t0);
           acc += pv0;
           pv0 = __ldcg(table + pair(t0, 0, n));
-          if (kDual) {
-            acc += pv1;
-            pv1 = __ldcg(table + pair(t0, 1, n));
-          }
+          acc += pv1;
+          pv1 = __ldcg(table + pair(t0, 1, n));
         }
         // move the leftover (< kG) entries to the front
         const int left = head - upto;
@@ -490,22 +482,33 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
         if (final_batch) break;
       }
       __syncwarp();
+      // the tile's energy: the last round's gathers, then the lane sums in a fixed shuffle order,
+      // into the tile's slot
+      acc += pv0;
+      acc += pv1;
+      pv0 = 0.0;
+      pv1 = 0.0;
+      double v = acc;
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (lane == 0) tsum[k] = v;
+      acc = 0.0;
     }
-    acc += pv0;
-    acc += pv1;
-    // counters, then the FP64 block reduction of the per-lane sums
+    // counters, then the pose energy: warp 0 adds the tile slots in a fixed order
     const unsigned wp = __reduce_add_sync(0xffffffffu, npairs);
     if (lane == 0) {
       if (wp) atomicAdd(&sh_cnt[3], (unsigned long long)wp);
       if (nevals) atomicAdd(&sh_cnt[4], (unsigned long long)nevals);
     }
-    double v = acc;
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (lane == 0) sh_red[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+      double v = 0.0;
+      for (int k = lane; k < ntiles; k += 32) v += tsum[k];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (lane == 0) sh_red[0] = v;
+    }
     __syncthreads();
     if (tid == 0) {
-      double E = 0.0;
-      for (int i = 0; i < kWarps; ++i) E += sh_red[i];
+      const double E = sh_red[0];
       const double score = ((E)*0.0157 - 4.7) * -1;
       C.scoring[p] = score;
       if (L.energy_out) L.energy_out[p] = E;
