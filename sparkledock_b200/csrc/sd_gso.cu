@@ -17,6 +17,8 @@
 // step can be replayed from a CUDA graph.
 #include <cuda_runtime.h>
 
+#include <string>
+
 #include "sd_crmath.h"
 #include "sd_internal.h"
 
@@ -256,4 +258,30 @@ int gso_launch(const GsoLaunch& L, int threads, cudaStream_t st) {
   return cudaGetLastError() == cudaSuccess ? SD_OK : SD_ERR_CUDA;
 }
 
+// the slerp's correctly rounded functions evaluated on the device (parity checking): fn 0 acos,
+// fn 1 sin
+__global__ void crmath_eval_kernel(int fn, const double* x, long long n, double* out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = fn == 0 ? sd_acos_cr(x[i]) : sd_sin_cr(x[i]);
+}
+
 }  // namespace sd
+
+extern "C" int sd_crmath_eval(int device, int fn, const double* x, long long n, double* out) {
+  if ((fn != 0 && fn != 1) || n < 0 || (n > 0 && (!x || !out))) return sd::fail(SD_ERR_ARG, "sd_crmath_eval: bad arguments");
+  if (n == 0) return SD_OK;
+  if (cudaSetDevice(device) != cudaSuccess) return sd::fail(SD_ERR_CUDA, "sd_crmath_eval: bad device");
+  double* d = nullptr;
+  if (cudaMalloc(&d, (size_t)n * 2 * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    return sd::fail(SD_ERR_OOM, "sd_crmath_eval: cudaMalloc failed");
+  }
+  cudaError_t e = cudaMemcpy(d, x, (size_t)n * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    sd::crmath_eval_kernel<<<148 * 8, 256>>>(fn, d, n, d + n);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out, d + n, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  return e == cudaSuccess ? SD_OK : sd::fail(SD_ERR_CUDA, std::string("sd_crmath_eval: ") + cudaGetErrorString(e));
+}
