@@ -145,70 +145,110 @@ static void atoms(or_mt64* r, int n, int* type, double* charge, int* lj, int* ma
   for (int i = 0; i < n; ++i) mask[i] = u01(r) < 0.03 ? 0 : 1;
 }
 
-/* Khachiyan minimum-volume enclosing ellipsoid centre, tolerance tol: weights u, X = sum u q q^T
- * (q = [p, 1]), Gauss-Jordan inverse with partial pivoting, the point of largest q^T X^-1 q
- * gains weight step = (m - d - 1) / ((d + 1)(m - 1)), until the weight change is below tol. */
+/* 4x4 inverse, column-major in and out, in the operation order of the reference's Eigen build of
+ * MatrixXd::inverse() (Eigen 3.4 vendored with the reference: PartialPivLU, unblocked for this
+ * size, then triangular solves of P I): see or_mvee_center. */
+static void lu_inverse4(const double* in, double* out) {
+  double m[4][4]; /* m[c][r] */
+  int t[4];
+  memcpy(m, in, sizeof m);
+  for (int k = 0; k < 4; ++k) {
+    int p = k;
+    for (int r = k + 1; r < 4; ++r)
+      if (fabs(m[k][r]) > fabs(m[k][p])) p = r;
+    t[k] = p;
+    if (fabs(m[k][p]) != 0.0) {
+      if (p != k)
+        for (int c = 0; c < 4; ++c) {
+          const double v = m[c][k];
+          m[c][k] = m[c][p];
+          m[c][p] = v;
+        }
+      for (int r = k + 1; r < 4; ++r) m[k][r] = m[k][r] / m[k][k];
+    }
+    for (int c = k + 1; c < 4; ++c)
+      for (int r = k + 1; r < 4; ++r) m[c][r] = m[c][r] - m[k][r] * m[c][k];
+  }
+  double x[4][4]; /* x[c][r] */
+  for (int c = 0; c < 4; ++c)
+    for (int r = 0; r < 4; ++r) x[c][r] = c == r ? 1.0 : 0.0;
+  for (int k = 0; k < 4; ++k)
+    for (int c = 0; c < 4; ++c) {
+      const double v = x[c][k];
+      x[c][k] = x[c][t[k]];
+      x[c][t[k]] = v;
+    }
+  /* unit lower, forward */
+  for (int k = 0; k < 4; ++k)
+    for (int c = 0; c < 4; ++c)
+      for (int r = k + 1; r < 4; ++r) x[c][r] = x[c][r] - x[c][k] * m[k][r];
+  /* upper, backward: multiply by the reciprocal of the diagonal */
+  for (int k = 3; k >= 0; --k) {
+    const double rd = 1.0 / m[k][k];
+    for (int c = 0; c < 4; ++c) {
+      x[c][k] = x[c][k] * rd;
+      for (int r = 0; r < k; ++r) x[c][r] = x[c][r] - x[c][k] * m[k][r];
+    }
+  }
+  memcpy(out, x, sizeof x);
+}
+
+/* Khachiyan minimum-volume enclosing ellipsoid centre, tolerance tol, restating the reference's
+ * minimum_volume_ellipsoid (source/dock/src/prepare_gso_tasks.cc:106-267, with its matrix helpers
+ * at :71-104, run on one thread) operation for operation: weights u = 1/N; per iteration
+ * V[a][b] = sum_i q_i[a] (q_i[b] u_i) over ascending atoms (q = [p, 1]); the inverse of the
+ * column-major matrix with data V (lu_inverse4); m_i = sum_k q_i[k] (sum_c Ainv(c,k) q_i[c]);
+ * the first atom of largest m_i > 0 gains weight step = ((m - 3) - 1) / (4 (m - 1)) while the
+ * others shrink by (1 - step); the weight change's 2-norm ends the loop below tol; the centre is
+ * sum_i p_i u_i. */
 void or_mvee_center(const double* p, int n, double tol, double* center) {
   double* u = (double*)malloc(sizeof(double) * n);
+  double* un = (double*)malloc(sizeof(double) * n);
   for (int i = 0; i < n; ++i) u[i] = 1.0 / n;
   double err = 1 + tol;
-  int it = 0;
-  while (err > tol && it < 100000) {
-    ++it;
-    double X[4][4];
-    memset(X, 0, sizeof X);
-    for (int i = 0; i < n; ++i) {
-      const double q[4] = {p[i * 3], p[i * 3 + 1], p[i * 3 + 2], 1.0};
-      for (int a = 0; a < 4; ++a)
-        for (int b = 0; b < 4; ++b) X[a][b] += u[i] * q[a] * q[b];
-    }
-    double A[4][8];
+  for (int it = 0; err > tol && it < 100000; ++it) {
+    double V[16];
     for (int a = 0; a < 4; ++a)
-      for (int b = 0; b < 8; ++b) A[a][b] = b < 4 ? X[a][b] : (b - 4 == a ? 1.0 : 0.0);
-    for (int c = 0; c < 4; ++c) {
-      int piv = c;
-      for (int a = c + 1; a < 4; ++a)
-        if (fabs(A[a][c]) > fabs(A[piv][c])) piv = a;
-      for (int b = 0; b < 8; ++b) {
-        const double t = A[c][b];
-        A[c][b] = A[piv][b];
-        A[piv][b] = t;
-      }
-      const double d = A[c][c];
-      for (int b = 0; b < 8; ++b) A[c][b] /= d;
-      for (int a = 0; a < 4; ++a)
-        if (a != c) {
-          const double f = A[a][c];
-          for (int b = 0; b < 8; ++b) A[a][b] -= f * A[c][b];
+      for (int b = 0; b < 4; ++b) {
+        double acc = 0.0;
+        for (int i = 0; i < n; ++i) {
+          const double qa = a < 3 ? p[i * 3 + a] : 1.0, qb = b < 3 ? p[i * 3 + b] : 1.0;
+          acc += qa * (qb * u[i]);
         }
-    }
-    double mx = -1;
-    int j = 0;
+        V[a * 4 + b] = acc;
+      }
+    double inv[16];
+    lu_inverse4(V, inv);
+    int best = 0;
+    double top = 0.0;
     for (int i = 0; i < n; ++i) {
       const double q[4] = {p[i * 3], p[i * 3 + 1], p[i * 3 + 2], 1.0};
-      double m = 0;
-      for (int a = 0; a < 4; ++a)
-        for (int b = 0; b < 4; ++b) m += q[a] * A[a][4 + b] * q[b];
-      if (m > mx) {
-        mx = m;
-        j = i;
+      double m = 0.0;
+      for (int k = 0; k < 4; ++k) {
+        double y = 0.0;
+        for (int c = 0; c < 4; ++c) y += inv[k * 4 + c] * q[c];
+        m += q[k] * y;
+      }
+      if (m > top) {
+        top = m;
+        best = i;
       }
     }
-    const double step = (mx - 3 - 1.0) / ((3 + 1.0) * (mx - 1.0));
-    double e2 = 0;
-    for (int i = 0; i < n; ++i) {
-      const double nu = (1.0 - step) * u[i] + (i == j ? step : 0.0);
-      e2 += (nu - u[i]) * (nu - u[i]);
-      u[i] = nu;
-    }
+    const double step = (top - 3 - 1.0) / ((3 + 1.0) * (top - 1.0));
+    for (int i = 0; i < n; ++i) un[i] = (1.0 - step) * u[i];
+    un[best] += step;
+    double e2 = 0.0;
+    for (int i = 0; i < n; ++i) e2 += (un[i] - u[i]) * (un[i] - u[i]);
     err = sqrt(e2);
+    for (int i = 0; i < n; ++i) u[i] = un[i];
   }
   for (int d = 0; d < 3; ++d) {
-    double c = 0;
+    double c = 0.0;
     for (int i = 0; i < n; ++i) c += p[i * 3 + d] * u[i];
     center[d] = c;
   }
   free(u);
+  free(un);
 }
 
 static void starting_poses(or_mt64* rs, const double* rec, int nr, int S, int G, int nmr, int nml, double* poses) {

@@ -134,6 +134,10 @@ double or_acos_cr(double x) {
   return a.hi + a.lo;
 }
 
+void or_crmath_eval(int fn, const double* x, long long n, double* out) {
+  for (long long i = 0; i < n; ++i) out[i] = fn == 0 ? or_acos_cr(x[i]) : or_sin_cr(x[i]);
+}
+
 /* ---------------------------------------------------------------------------------------
  * Pose transforms.
  * receptor: r = r0 + sum_j mask * mode_j * ext_j  (prepare_gso_tasks.cc:458, :465-482)

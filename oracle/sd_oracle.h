@@ -95,6 +95,8 @@ void or_cluster(const or_system* sys, const double* pos, const double* scores, c
                 const int* lig_bb, int* n_clusters, int* rep, int* size, int* member);
 double or_sin_cr(double x);
 double or_acos_cr(double x);
+/* out[i] = or_acos_cr(x[i]) (fn 0) or or_sin_cr(x[i]) (fn 1) */
+void or_crmath_eval(int fn, const double* x, long long n, double* out);
 /* slerp of the reference (prepare_gso_tasks.cc:1370-1421) with cr or libm math */
 void or_slerp(double* self, double* other, double step, int cr_math);
 

@@ -104,9 +104,6 @@ void atoms(Rng& r, int n, int* type, double* charge, int* lj, int* mask) {
 
 }  // namespace
 
-// Khachiyan's minimum-volume enclosing ellipsoid centre (the ligand reference point of
-// prepare_gso_tasks.cc:106-267 / :1196-1202, tolerance 0.01 as at :1196).  Only the diagonal
-// q_i^T X^-1 q_i is formed, O(N) per iteration.
 // Starting poses: swarm centres at independent uniform directions on a shell 10 A outside the
 // receptor's bounding sphere (receptor centred at the origin), each glowworm at its centre plus
 // N(0, 2 A) per axis, a uniform random unit quaternion (Shoemake) and N(0, 1) ANM extents.
@@ -142,58 +139,114 @@ void starting_poses(Rng& rs, const double* rec_xyz, int n_rec, int S, int G, int
   }
 }
 
+namespace {
+
+// Inverse of a 4x4 matrix (column-major, a[c*4 + r]) in the operation order of the reference's
+// MatrixXd::inverse() (its vendored Eigen 3.4: PartialPivLU, then solve against the identity):
+//  * LU with partial pivoting, column by column: pivot = first row of largest |a(r,k)|, rows
+//    swapped, the column below divided by the pivot, then a(r,c) -= a(r,k) * a(k,c);
+//  * X = P I (the same row swaps applied to the identity);
+//  * unit-lower solve, top to bottom: X(r,j) -= X(k,j) * L(r,k) for r > k;
+//  * upper solve, bottom to top: X(i,j) *= 1 / U(i,i), then X(r,j) -= X(i,j) * U(r,i) for r < i.
+void inverse4_lu(const double* a, double* x) {
+  double lu[16];
+  for (int k = 0; k < 16; ++k) lu[k] = a[k];
+  int piv[4];
+  for (int k = 0; k < 4; ++k) {
+    int p = k;
+    double best = std::fabs(lu[k * 4 + k]);
+    for (int r = k + 1; r < 4; ++r)
+      if (std::fabs(lu[k * 4 + r]) > best) {
+        best = std::fabs(lu[k * 4 + r]);
+        p = r;
+      }
+    piv[k] = p;
+    if (best != 0.0) {
+      if (p != k)
+        for (int c = 0; c < 4; ++c) std::swap(lu[c * 4 + k], lu[c * 4 + p]);
+      for (int r = k + 1; r < 4; ++r) lu[k * 4 + r] /= lu[k * 4 + k];
+    }
+    for (int c = k + 1; c < 4; ++c)
+      for (int r = k + 1; r < 4; ++r) lu[c * 4 + r] -= lu[c * 4 + k] * lu[k * 4 + r];
+  }
+  for (int k = 0; k < 16; ++k) x[k] = (k % 5 == 0) ? 1.0 : 0.0;
+  for (int k = 0; k < 4; ++k)
+    if (piv[k] != k)
+      for (int c = 0; c < 4; ++c) std::swap(x[c * 4 + k], x[c * 4 + piv[k]]);
+  for (int k = 0; k < 4; ++k)
+    for (int j = 0; j < 4; ++j) {
+      const double b = x[j * 4 + k];
+      for (int r = k + 1; r < 4; ++r) x[j * 4 + r] -= b * lu[k * 4 + r];
+    }
+  for (int i = 3; i >= 0; --i) {
+    const double inv = 1.0 / lu[i * 4 + i];
+    for (int j = 0; j < 4; ++j) {
+      x[j * 4 + i] *= inv;
+      const double b = x[j * 4 + i];
+      for (int r = 0; r < i; ++r) x[j * 4 + r] -= b * lu[i * 4 + r];
+    }
+  }
+}
+
+}  // namespace
+
+// Khachiyan's minimum-volume enclosing ellipsoid centre with tolerance tol, in the operation
+// order of the reference's minimum_volume_ellipsoid (prepare_gso_tasks.cc:106-267, with its
+// helpers multiplyDiagonalMatrix / multiplyMatrices / transpose, :71-104, one thread), so the
+// centre is bit-identical to the reference's:
+//   q_i = (x_i, y_i, z_i, 1), u_i = 1/N;  V[a][b] = sum_i q_i[a] * (q_i[b] * u_i) (ascending i);
+//   A = the 4x4 matrix whose column-major data is V, inverted as above;
+//   m_i = sum_k q_i[k] * (sum_m Ainv(m, k) * q_i[m]);  j = first index of the largest m_i (> 0);
+//   step = ((m_j - 3) - 1) / (4 (m_j - 1));  u <- (1 - step) u, u_j += step;
+//   error = sqrt(sum_i (u_new - u_old)^2);  repeat while error > tol;
+//   centre[d] = sum_i p_i[d] * u_i.
+// Only the diagonal m_i of the reference's N x N product is formed (each entry is computed the
+// same way whether or not the rest of the matrix is), O(N) per iteration.
 void mvee_center(const double* p, int n, double tol, double* center) {
-  std::vector<double> u(n, 1.0 / n);
+  std::vector<double> u(n, 1.0 / n), nu(n), w((size_t)4 * n);
   double err = 1 + tol;
   int it = 0;
+  auto q = [&](int i, int a) { return a == 3 ? 1.0 : p[(size_t)i * 3 + a]; };
   while (err > tol && it < 100000) {
     ++it;
-    double X[4][4] = {};
-    for (int i = 0; i < n; ++i) {
-      double q[4] = {p[i * 3], p[i * 3 + 1], p[i * 3 + 2], 1.0};
-      for (int a = 0; a < 4; ++a)
-        for (int b = 0; b < 4; ++b) X[a][b] += u[i] * q[a] * q[b];
-    }
-    // invert 4x4 by Gauss-Jordan
-    double A[4][8];
+    double V[16];
     for (int a = 0; a < 4; ++a)
-      for (int b = 0; b < 8; ++b) A[a][b] = b < 4 ? X[a][b] : (b - 4 == a ? 1.0 : 0.0);
-    for (int c = 0; c < 4; ++c) {
-      int piv = c;
-      for (int a = c + 1; a < 4; ++a)
-        if (std::fabs(A[a][c]) > std::fabs(A[piv][c])) piv = a;
-      for (int b = 0; b < 8; ++b) std::swap(A[c][b], A[piv][b]);
-      double d = A[c][c];
-      for (int b = 0; b < 8; ++b) A[c][b] /= d;
-      for (int a = 0; a < 4; ++a)
-        if (a != c) {
-          double f = A[a][c];
-          for (int b = 0; b < 8; ++b) A[a][b] -= f * A[c][b];
-        }
-    }
-    double mx = -1;
+      for (int i = 0; i < n; ++i) w[(size_t)a * n + i] = q(i, a) * u[i];
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 4; ++b) {
+        double sum = 0.0;
+        for (int i = 0; i < n; ++i) sum += q(i, a) * w[(size_t)b * n + i];
+        V[a * 4 + b] = sum;
+      }
+    double X[16];
+    inverse4_lu(V, X);
+    double mx = 0.0;
     int j = 0;
     for (int i = 0; i < n; ++i) {
-      double q[4] = {p[i * 3], p[i * 3 + 1], p[i * 3 + 2], 1.0}, m = 0;
-      for (int a = 0; a < 4; ++a)
-        for (int b = 0; b < 4; ++b) m += q[a] * A[a][4 + b] * q[b];
+      double t[4];
+      for (int k = 0; k < 4; ++k) {
+        double sum = 0.0;
+        for (int m = 0; m < 4; ++m) sum += X[k * 4 + m] * q(i, m);
+        t[k] = sum;
+      }
+      double m = 0.0;
+      for (int k = 0; k < 4; ++k) m += q(i, k) * t[k];
       if (m > mx) {
         mx = m;
         j = i;
       }
     }
-    double step = (mx - 3 - 1.0) / ((3 + 1.0) * (mx - 1.0));
-    double e2 = 0;
-    for (int i = 0; i < n; ++i) {
-      double nu = (1.0 - step) * u[i] + (i == j ? step : 0.0);
-      e2 += (nu - u[i]) * (nu - u[i]);
-      u[i] = nu;
-    }
+    const double step = (mx - 3 - 1.0) / ((3 + 1.0) * (mx - 1.0));
+    for (int i = 0; i < n; ++i) nu[i] = (1.0 - step) * u[i];
+    nu[j] += step;
+    double e2 = 0.0;
+    for (int i = 0; i < n; ++i) e2 += (nu[i] - u[i]) * (nu[i] - u[i]);
     err = std::sqrt(e2);
+    u.swap(nu);
   }
   for (int d = 0; d < 3; ++d) {
-    double c = 0;
-    for (int i = 0; i < n; ++i) c += p[i * 3 + d] * u[i];
+    double c = 0.0;
+    for (int i = 0; i < n; ++i) c += p[(size_t)i * 3 + d] * u[i];
     center[d] = c;
   }
 }

@@ -84,6 +84,7 @@ def oracle():
         L.or_synth_generate.argtypes = [C.c_int] * 6 + [C.c_ulonglong, C.POINTER(OrSynthOut)]
         L.or_synth_tables.argtypes = [C.c_ulonglong, _dp, _dp, _dp]
         L.or_mvee_center.argtypes = [_dp, C.c_int, C.c_double, _dp]
+        L.or_crmath_eval.argtypes = [C.c_int, _dp, C.c_longlong, _dp]
         _oracle = L
     return _oracle
 

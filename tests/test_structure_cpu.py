@@ -118,18 +118,25 @@ def test_starting_poses_match_synthetic_generator():
 
 @needs_ref
 def test_reference_point_matches_reference_ellipsoid():
-    """sd_reference_point (Khachiyan MVEE centre, tolerance 0.01) against the reference's own
-    minimum_volume_ellipsoid: within 1e-12 (the iteration is restated with its own linear algebra,
-    not Eigen's, so the last bits may differ) on random point clouds and the shipped ligands."""
+    """sd_reference_point (Khachiyan MVEE centre, tolerance 0.01, restated in the operation order of
+    the reference's minimum_volume_ellipsoid and of the Eigen inverse it calls) is bit-identical to
+    the reference's own compiled function on random point clouds of many shapes and sizes and on every
+    ligand of the benchmark structures shipped with the reference; so is the oracle's independent
+    restatement.  The reference runs single-threaded here (NUM_THREADS unset): with more threads
+    its weight-change sum is a data race."""
     import ctypes as C
-    from oracle_bind import ref
+    from oracle_bind import oracle, ref
     dp = C.POINTER(C.c_double)
     rng = np.random.default_rng(0)
-    clouds = [np.ascontiguousarray(rng.normal(size=(int(rng.integers(50, 1500)), 3)) * rng.uniform(5, 20, 3))
-              for _ in range(10)]
+    clouds = [np.ascontiguousarray(rng.normal(size=(int(rng.integers(4, 1500)), 3)) * rng.uniform(0.5, 30, 3) +
+                                   rng.uniform(-50, 50, 3)) for _ in range(30)]
     clouds += [sd.Structure(p, sd.SD_PDB_NOXT | sd.SD_PDB_NOH | sd.SD_PDB_NOW).xyz for p in PDBS if "_l_" in p]
+    assert len(clouds) == 40
     for pts in clouds:
-        a, c, poles = np.empty(3), np.empty(3), np.empty(18)
+        pts = np.ascontiguousarray(pts)
+        a, c, o, poles = np.empty(3), np.empty(3), np.empty(3), np.empty(18)
         assert sd._abi.lib().sd_reference_point(sd.dptr(pts), len(pts), sd.dptr(a)) == 0
         ref().ref_min_volume_ellipsoid(pts.ctypes.data_as(dp), len(pts), c.ctypes.data_as(dp), poles.ctypes.data_as(dp))
-        assert np.abs(a - c).max() <= 1e-12 * max(1.0, np.abs(c).max())
+        oracle().or_mvee_center(pts.ctypes.data_as(dp), len(pts), 0.01, o.ctypes.data_as(dp))
+        assert np.array_equal(a, c), (len(pts), a - c)
+        assert np.array_equal(o, c), (len(pts), o - c)
