@@ -131,12 +131,17 @@ struct sd_ctx {
   int max_nr = 0, max_nl = 0, max_G = 0;
   // stateless scratch
   DevBuf s_pose, s_score, s_ref, s_energy, s_work, s_grad, s_bins;
+  // per-CTA global scratch of the spill instantiations (complexes too large for shared memory)
+  DevBuf s_spill;
+  int smem_optin = 0;      // shared memory a CTA may use on this device (opt-in maximum)
   // step graph
   cudaGraphExec_t graph = nullptr;
   int graph_precision = -1;
   int score_threads = 256;
   int score_grid = 0;
   size_t score_smem = 0;
+  bool score_spill = false;  // the last configured scorer launch uses the spill instantiation
+  size_t spill_stride = 0;
   // autotuner state (mixed-precision DFIRE kernel variants)
   int mixed_variant = 0;
   bool tuned = false;
@@ -177,8 +182,8 @@ int alloc_dev(ComplexHost& h, size_t n, T** dst) {
 
 int check_desc(const sd_complex_desc& d, int scoring) {
   if (d.n_rec <= 0 || d.n_lig <= 0) return fail(SD_ERR_ARG, "complex: empty receptor or ligand");
-  if (d.n_rec > SD_MAX_REC) return fail(SD_ERR_ARG, "complex: receptor has more than 24576 atoms");
-  if (d.n_lig > SD_MAX_LIG) return fail(SD_ERR_ARG, "complex: ligand has more than 6144 atoms");
+  if (d.n_rec > SD_MAX_REC) return fail(SD_ERR_ARG, "complex: receptor has more than 4,194,304 atoms");
+  if (d.n_lig > SD_MAX_LIG) return fail(SD_ERR_ARG, "complex: ligand has more than 65,504 atoms");
   if (d.n_swarms <= 0 || d.n_glowworms <= 0 || d.n_glowworms > SD_MAX_G)
     return fail(SD_ERR_ARG, "complex: swarms must be > 0 and glowworms in 1..1024");
   if ((long long)d.n_swarms * d.n_glowworms >= (1 << 24))
@@ -435,10 +440,35 @@ int rebuild_worklist(sd_ctx* c) {
   return SD_OK;
 }
 
-int configure_score_v(sd_ctx* c, int precision, int variant, int* grid, size_t* smem) {
-  const size_t sm = score_smem_bytes(precision, c->scoring, c->max_nr, c->max_nl, variant);
-  const void* k = score_kernel_ptr(precision, c->scoring, variant);
-  const int threads = score_threads_of(precision, c->scoring, variant);
+// The spill scratch, grown to at least bytes.  The step graph holds the scratch's address, so a new
+// scratch means a new capture at the next step.
+int grow_spill(sd_ctx* c, size_t bytes) {
+  if (c->s_spill.bytes >= bytes) return SD_OK;
+  if (c->graph) {
+    cudaStreamSynchronize(c->stream);
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  return ensure(c, c->s_spill, bytes);
+}
+
+// Launch shape of the scorer on this context: persistent grid (resident CTAs x SMs), dynamic shared
+// memory, threads.  When the per-pose arrays of the largest complex do not fit in the shared memory
+// a CTA may use, the spill instantiation is chosen (no dynamic shared memory) and the context's
+// spill scratch is sized to grid x per-CTA bytes; alloc = false refuses that instead of allocating.
+int configure_score_v(sd_ctx* c, int precision, int variant, int* grid, size_t* smem, bool alloc = true) {
+  const size_t need = score_smem_bytes(precision, c->scoring, c->max_nr, c->max_nl, variant);
+  const void* k = score_kernel_ptr(precision, c->scoring, variant, false);
+  cudaFuncAttributes fa;
+  SD_CUDA(cudaFuncGetAttributes(&fa, k));
+  const bool spill = need + fa.sharedSizeBytes > (size_t)c->smem_optin;
+  size_t sm = need;
+  int threads = score_threads_of(precision, c->scoring, variant);
+  if (spill) {
+    k = score_kernel_ptr(precision, c->scoring, variant, true);
+    sm = 0;
+    threads = score_threads_spill(precision, c->scoring);
+  }
   SD_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(sm, 1)));
   int per_sm = 0;
   SD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, sm));
@@ -446,11 +476,28 @@ int configure_score_v(sd_ctx* c, int precision, int variant, int* grid, size_t* 
   *grid = per_sm * c->nsm;
   *smem = sm;
   c->score_threads = threads;
+  c->score_spill = spill;
+  if (spill) {
+    const size_t stride = (need + 255) & ~(size_t)255;
+    if (c->s_spill.bytes < stride * (size_t)*grid) {
+      if (!alloc) return fail(SD_ERR_NOTSUP, "complex too large for shared memory: its scorer needs the context's "
+                                             "global scratch, which this call may not allocate");
+      int rc = grow_spill(c, stride * (size_t)*grid);
+      if (rc) return rc;
+    }
+    c->spill_stride = stride;
+  }
   return SD_OK;
 }
 
-int configure_score(sd_ctx* c, int precision, int* grid, size_t* smem) {
-  return configure_score_v(c, precision, c->mixed_variant, grid, smem);
+int configure_score(sd_ctx* c, int precision, int* grid, size_t* smem, bool alloc = true) {
+  return configure_score_v(c, precision, c->mixed_variant, grid, smem, alloc);
+}
+
+// the spill scratch of the last configured launch (null pointers when it uses shared memory)
+void set_spill(const sd_ctx* c, ScoreLaunch& L) {
+  L.spill = c->score_spill ? (unsigned char*)c->s_spill.p : nullptr;
+  L.spill_stride = c->score_spill ? c->spill_stride : 0;
 }
 
 // Autotuner: times every compiled variant of the mixed DFIRE kernel (warps per CTA x resident
@@ -535,12 +582,17 @@ int autotune_mixed(sd_ctx* c) {
       c->tune_ms[v] = -1;
       continue;
     }
+    if (c->score_spill) {
+      // too large for shared memory: one spill instantiation, nothing to choose
+      c->tune_ms[v] = -1;
+      break;
+    }
     double vbest = 1e300;
     for (int rep = 0; rep < 3; ++rep) {
       ctl.grab[0] = ctl.grab[1] = 0;
       SD_CUDA(cudaMemcpyAsync(c->d_ctl_scratch, &ctl, sizeof ctl, cudaMemcpyHostToDevice, c->stream));
       SD_CUDA(cudaEventRecord(e0, c->stream));
-      if ((rc = score_launch(L, SD_PREC_MIXED, c->scoring, grid, c->score_threads, sm, c->stream, v)))
+      if ((rc = score_launch(L, SD_PREC_MIXED, c->scoring, grid, c->score_threads, sm, c->stream, v, false)))
         return fail(rc, std::string("autotune launch: ") + cudaGetErrorString(cudaGetLastError()));
       SD_CUDA(cudaEventRecord(e1, c->stream));
       SD_CUDA(cudaEventSynchronize(e1));
@@ -573,7 +625,9 @@ int enqueue_step(sd_ctx* c, int precision, int grid, size_t sm) {
   L.lj_eps = c->d_lj_eps;
   L.lj_sigma = c->d_lj_sigma;
   L.energy_out = nullptr;
-  if ((rc = score_launch(L, precision, c->scoring, grid, c->score_threads, sm, c->stream, c->mixed_variant)))
+  set_spill(c, L);
+  if ((rc = score_launch(L, precision, c->scoring, grid, c->score_threads, sm, c->stream, c->mixed_variant,
+                         c->score_spill)))
     return fail(rc, std::string("score kernel launch: ") + cudaGetErrorString(cudaGetLastError()));
   GsoLaunch G{};
   G.cplx = c->d_cplx;
@@ -609,10 +663,13 @@ int ctx_noalloc_view(sd_ctx* c, int ci, int precision, DevComplex* desc, ScoreLa
   if (precision < SD_PREC_FP64_REF || precision > SD_PREC_MIXED)
     return fail(SD_ERR_ARG, "sd_score_poses_noalloc: unknown precision");
   SD_CUDA(cudaSetDevice(c->device));
-  int rc = configure_score(c, precision, grid, smem);
+  // a complex too large for shared memory uses the context's spill scratch, allocated by an
+  // earlier allocating call; this call only uses it when it is already large enough
+  int rc = configure_score(c, precision, grid, smem, false);
   if (rc) return rc;
   *desc = c->cx[ci].d;
   memset(L, 0, sizeof *L);
+  set_spill(c, *L);
   L->table64 = c->d_table64;
   L->tablek = c->d_tablek;
   L->lj_eps = c->d_lj_eps;
@@ -689,6 +746,7 @@ int sd_ctx_create(const sd_complex_desc* complexes, int n_complexes, const sd_ta
   sd_ctx* c = new sd_ctx();
   c->device = device;
   c->nsm = prop.multiProcessorCount;
+  c->smem_optin = (int)prop.sharedMemPerBlockOptin;
   c->ncplx = n_complexes;
   c->scoring = scoring;
   c->precision = precision;
@@ -779,7 +837,7 @@ int sd_ctx_destroy(sd_ctx* c) {
     for (void* p : h.owned) cudaFree(p);
   void* ps[] = {c->d_cplx, c->d_cplx_scratch, c->d_table64, c->d_tablek, c->d_lj_eps, c->d_lj_sigma, c->d_ctl,
                 c->d_ctl_scratch, c->d_work[0], c->d_work[1], c->d_swarm_map, c->s_pose.p, c->s_score.p,
-                c->s_ref.p, c->s_energy.p, c->s_work.p, c->s_grad.p, c->s_bins.p};
+                c->s_ref.p, c->s_energy.p, c->s_work.p, c->s_grad.p, c->s_bins.p, c->s_spill.p};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -1032,7 +1090,9 @@ int sd_score_poses(sd_ctx* c, int ci, const double* poses, int n, int precision,
   L.lj_eps = c->d_lj_eps;
   L.lj_sigma = c->d_lj_sigma;
   L.energy_out = (double*)c->s_energy.p;
-  if ((rc = score_launch(L, precision, c->scoring, grid, c->score_threads, sm, c->stream, c->mixed_variant)))
+  set_spill(c, L);
+  if ((rc = score_launch(L, precision, c->scoring, grid, c->score_threads, sm, c->stream, c->mixed_variant,
+                         c->score_spill)))
     return fail(rc, std::string("score kernel: ") + cudaGetErrorString(cudaGetLastError()));
   SD_CUDA(cudaMemcpyAsync(score_out, c->s_score.p, (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));
   if (energy_out)
@@ -1099,13 +1159,23 @@ int sd_pydock_grad(sd_ctx* c, int ci, const double* poses, int n, int precision,
   SD_CUDA(cudaMemcpyAsync(c->s_work.p, work.data(), (size_t)n * 4, cudaMemcpyHostToDevice, c->stream));
   SD_CUDA(cudaMemcpyAsync(&c->d_cplx_scratch[ci], &S, sizeof S, cudaMemcpyHostToDevice, c->stream));
   SD_CUDA(cudaMemcpyAsync(c->d_ctl_scratch, &ctl, sizeof ctl, cudaMemcpyHostToDevice, c->stream));
-  const size_t sm = pydock_smem_bytes(precision, true, c->max_nl, c->max_nr);
-  const void* k = pydock_kernel_ptr(precision, true);
-  SD_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const size_t need = pydock_smem_bytes(precision, true, c->max_nl, c->max_nr);
+  const void* k = pydock_kernel_ptr(precision, true, false);
+  cudaFuncAttributes fa;
+  SD_CUDA(cudaFuncGetAttributes(&fa, k));
+  // a ligand too large for shared memory: the spill instantiation, per-CTA arrays in global scratch
+  const bool spill = need + fa.sharedSizeBytes > (size_t)c->smem_optin;
+  const size_t sm = spill ? 0 : need;
+  if (spill) k = pydock_kernel_ptr(precision, true, true);
+  SD_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(sm, 1)));
   int per_sm = 0;
   SD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, pydock_threads(), sm));
-  if (per_sm < 1) return fail(SD_ERR_ARG, "pyDock gradient kernel does not fit on an SM (shared memory)");
+  if (per_sm < 1) return fail(SD_ERR_ARG, "pyDock gradient kernel does not fit on an SM");
+  const size_t stride = (need + 255) & ~(size_t)255;
+  if (spill && (rc = grow_spill(c, stride * (size_t)per_sm * c->nsm))) return rc;
   ScoreLaunch L{};
+  L.spill = spill ? (unsigned char*)c->s_spill.p : nullptr;
+  L.spill_stride = spill ? stride : 0;
   L.cplx = c->d_cplx_scratch;
   L.ctl = c->d_ctl_scratch;
   L.work[0] = (const int*)c->s_work.p;
@@ -1115,7 +1185,7 @@ int sd_pydock_grad(sd_ctx* c, int ci, const double* poses, int n, int precision,
   L.lj_eps = c->d_lj_eps;
   L.lj_sigma = c->d_lj_sigma;
   L.energy_out = (double*)c->s_energy.p;
-  if ((rc = pydock_launch(L, precision, true, (double*)c->s_grad.p, per_sm * c->nsm, sm, c->stream)))
+  if ((rc = pydock_launch(L, precision, true, (double*)c->s_grad.p, per_sm * c->nsm, sm, c->stream, spill)))
     return fail(rc, std::string("pyDock gradient kernel: ") + cudaGetErrorString(cudaGetLastError()));
   if (energy_out)
     SD_CUDA(cudaMemcpyAsync(energy_out, c->s_energy.p, (size_t)n * 8, cudaMemcpyDeviceToHost, c->stream));

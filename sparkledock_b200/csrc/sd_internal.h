@@ -21,8 +21,8 @@
 #define SD_CUTOFF2 225.0
 #define SD_MAX_COMPLEX 32
 #define SD_TILE 32              /* receptor atoms per tile (one warp lane each) */
-#define SD_MAX_LIG 6144         /* ligand atoms held in shared memory per pose */
-#define SD_MAX_REC 24576        /* receptor atoms (FP64 per-atom partials in shared memory) */
+#define SD_MAX_LIG 65504        /* ligand atoms: the mixed scorer's 16-bit ligand slot indices */
+#define SD_MAX_REC (1 << 22)    /* receptor atoms */
 #define SD_MAX_G 1024           /* glowworms per swarm (one thread each) */
 #define SD_CULL_MARGIN 0.05f    /* A, covers FP32 rounding of the conservative culling tests */
 #define SD_MAX_VARIANTS 16      /* compiled variants of the mixed DFIRE kernel (autotuner) */
@@ -138,6 +138,10 @@ struct ScoreLaunch {
   const double* lj_eps;    // [20] pyDock
   const double* lj_sigma;
   double* energy_out;      // nullable [local glowworm] raw energies (stateless scoring)
+  // per-CTA global scratch that replaces the dynamic shared memory of the spill instantiations
+  // (complexes whose per-pose arrays do not fit in shared memory); null otherwise
+  unsigned char* spill;
+  size_t spill_stride;     // bytes per CTA
 };
 
 struct GsoLaunch {
@@ -151,11 +155,13 @@ struct GsoLaunch {
 };
 
 // kernel launchers (sd_score.cu, sd_gso.cu)
+// spill: the instantiation that keeps its per-pose arrays in L.spill instead of shared memory
 int score_launch(const ScoreLaunch& L, int precision, int scoring, int grid, int threads, size_t smem,
-                 cudaStream_t st, int variant);
+                 cudaStream_t st, int variant, bool spill);
 size_t score_smem_bytes(int precision, int scoring, int max_nr, int max_nl, int variant);
 int score_threads_of(int precision, int scoring, int variant);
-const void* score_kernel_ptr(int precision, int scoring, int variant);
+int score_threads_spill(int precision, int scoring);
+const void* score_kernel_ptr(int precision, int scoring, int variant, bool spill);
 int mixed_variant_count();
 int mixed_variant_warps(int v);
 int mixed_variant_min_blocks(int v);
@@ -163,9 +169,9 @@ int gso_launch(const GsoLaunch& L, int threads, cudaStream_t st);
 int bins_launch(const DevComplex* cplx, int c, const double* d_pose, int precision, int* d_bins, int nr, int nl,
                 int* d_fallback, cudaStream_t st);
 size_t pydock_smem_bytes(int precision, bool grad, int max_nl, int max_nr);
-const void* pydock_kernel_ptr(int precision, bool grad);
+const void* pydock_kernel_ptr(int precision, bool grad, bool spill);
 int pydock_launch(const ScoreLaunch& L, int precision, bool grad, double* out_grad, int grid, size_t smem,
-                  cudaStream_t st);
+                  cudaStream_t st, bool spill);
 int pydock_threads();
 void set_key_thresholds(const double* t64);
 size_t cluster_smem_bytes(int G, int nbb);

@@ -174,8 +174,10 @@ extern "C" int sd_score_poses_noalloc(sd_ctx* ctx, int complex_idx, const double
   L.work[0] = reinterpret_cast<const int*>(scratch + kCtlBytes + kDescBytes);
   L.work[1] = L.work[0];
   L.energy_out = d_energy;
-  if ((rc = score_launch(L, precision, scoring, grid, score_threads_of(precision, scoring, variant), smem, stream,
-                         variant)))
+  const bool spill = L.spill != nullptr;
+  if ((rc = score_launch(L, precision, scoring, grid,
+                         spill ? score_threads_spill(precision, scoring) : score_threads_of(precision, scoring, variant),
+                         smem, stream, variant, spill)))
     return fail(rc, std::string("sd_score_poses_noalloc: scoring kernel: ") + cudaGetErrorString(cudaGetLastError()));
   if (sync) {
     unsigned long long bad = 0;

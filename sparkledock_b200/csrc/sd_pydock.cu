@@ -93,10 +93,12 @@ __device__ __forceinline__ T warp_sum(T v) {
 }  // namespace
 
 // out_grad: nullable [n][6 + nmr + nml] (GRAD), energies go to C.scoring as score (-E) and to
-// L.energy_out (E) when set
-template <class T, bool GRAD>
+// L.energy_out (E) when set.  kSpill: the per-pose arrays live in this CTA's slice of the global
+// scratch L.spill instead of shared memory (ligands too large for it).
+template <class T, bool GRAD, bool kSpill>
 __global__ void __launch_bounds__(kPdWarps * 32) pydock_kernel(ScoreLaunch L, double* out_grad) {
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  unsigned char* const smem = kSpill ? L.spill + (size_t)blockIdx.x * L.spill_stride : smem_dyn;
   __shared__ double sh_pose[7 + 2 * SD_MAX_MODES];
   __shared__ double sh_q[4], sh_qi[4];
   __shared__ LjPair<T> sh_lj[SD_LJ_TYPES * SD_LJ_TYPES];
@@ -428,22 +430,22 @@ size_t pydock_smem_bytes(int precision, bool grad, int max_nl, int max_nr) {
   return ts * nls * (4 + (grad ? 3 : 0)) + 16 * nlc + 4 * nls * 2 + 4 * ((max_nr + SD_TILE - 1) / SD_TILE) + 16;
 }
 
-const void* pydock_kernel_ptr(int precision, bool grad) {
-  if (precision == SD_PREC_MIXED)
-    return grad ? (const void*)pydock_kernel<float, true> : (const void*)pydock_kernel<float, false>;
-  return grad ? (const void*)pydock_kernel<double, true> : (const void*)pydock_kernel<double, false>;
+const void* pydock_kernel_ptr(int precision, bool grad, bool spill) {
+  if (precision == SD_PREC_MIXED) {
+    if (spill) return grad ? (const void*)pydock_kernel<float, true, true> : (const void*)pydock_kernel<float, false, true>;
+    return grad ? (const void*)pydock_kernel<float, true, false> : (const void*)pydock_kernel<float, false, false>;
+  }
+  if (spill) return grad ? (const void*)pydock_kernel<double, true, true> : (const void*)pydock_kernel<double, false, true>;
+  return grad ? (const void*)pydock_kernel<double, true, false> : (const void*)pydock_kernel<double, false, false>;
 }
 
 int pydock_launch(const ScoreLaunch& L, int precision, bool grad, double* out_grad, int grid, size_t smem,
-                  cudaStream_t st) {
-  const int threads = kPdWarps * 32;
-  if (precision == SD_PREC_MIXED) {
-    if (grad) pydock_kernel<float, true><<<grid, threads, smem, st>>>(L, out_grad);
-    else pydock_kernel<float, false><<<grid, threads, smem, st>>>(L, out_grad);
-  } else {
-    if (grad) pydock_kernel<double, true><<<grid, threads, smem, st>>>(L, out_grad);
-    else pydock_kernel<double, false><<<grid, threads, smem, st>>>(L, out_grad);
-  }
+                  cudaStream_t st, bool spill) {
+  ScoreLaunch l = L;
+  void* args[] = {(void*)&l, (void*)&out_grad};
+  if (cudaLaunchKernel(pydock_kernel_ptr(precision, grad, spill), dim3(grid), dim3(kPdWarps * 32), args,
+                       spill ? 0 : smem, st) != cudaSuccess)
+    return SD_ERR_CUDA;
   return cudaGetLastError() == cudaSuccess ? SD_OK : SD_ERR_CUDA;
 }
 

@@ -66,11 +66,14 @@ __device__ __forceinline__ int exact_key(double d2, const double* T) {
 // PREC: SD_PREC_FP64_REF (no culling) or SD_PREC_FP64 (culled); the mixed-precision kernel is
 // in sd_score_mixed.cuh.  16 warps per CTA: the per-pose shared memory (receptor accumulators,
 // ligand atoms) allows two CTAs per SM, so the warps per CTA set the SM's residency.
+// kSpill: the per-pose arrays live in this CTA's slice of the global scratch L.spill instead
+// (complexes too large for shared memory); the arithmetic is the same.
 constexpr int kFp64Threads = 512;
 
-template <int PREC>
+template <int PREC, bool kSpill>
 __global__ void __launch_bounds__(kFp64Threads) dfire_score_kernel(ScoreLaunch L) {
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  unsigned char* const smem = kSpill ? L.spill + (size_t)blockIdx.x * L.spill_stride : smem_dyn;
   __shared__ double sh_pose[7 + 2 * SD_MAX_MODES];
   __shared__ double sh_q[4], sh_qi[4];
   __shared__ double sh_T[32];
@@ -305,13 +308,17 @@ struct MixedVariant {
   int warps;
   int min_blocks;
 };
-#define SD_MIXED(W, B) { (const void*)dfire_score_mixed_kernel<W, B>, W, B }
+#define SD_MIXED(W, B) { (const void*)dfire_score_mixed_kernel<W, B, false>, W, B }
 // variant 0 (the default before the autotuner has run) is the fastest measured on the
 // 3002 / 1274-atom workload.  The variants give bit-identical energies (same per-tile work and
 // summation order), so the tuner's choice never changes a result.
 static const MixedVariant kMixedVariants[] = {
     SD_MIXED(8, 3), SD_MIXED(4, 5), SD_MIXED(4, 4), SD_MIXED(8, 2),
 };
+// the spill instantiation of the mixed kernel: variant 0's shape (the per-tile work, and so every
+// energy, is the same in every variant)
+static const MixedVariant kMixedSpill = {(const void*)dfire_score_mixed_kernel<8, 3, true>, 8, 3};
+
 constexpr int kNumMixedVariants = sizeof(kMixedVariants) / sizeof(kMixedVariants[0]);
 static_assert(kNumMixedVariants <= SD_MAX_VARIANTS, "variant table");
 
@@ -338,28 +345,33 @@ int score_threads_of(int precision, int scoring, int variant) {
   return precision == SD_PREC_MIXED ? mixed_variant_warps(variant) * 32 : kFp64Threads;
 }
 
-const void* score_kernel_ptr(int precision, int scoring, int variant) {
-  if (scoring == SD_SCORING_PYDOCK) return pydock_kernel_ptr(precision, false);
+int score_threads_spill(int precision, int scoring) {
+  if (scoring == SD_SCORING_PYDOCK) return pydock_threads();
+  return precision == SD_PREC_MIXED ? kMixedSpill.warps * 32 : kFp64Threads;
+}
+
+const void* score_kernel_ptr(int precision, int scoring, int variant, bool spill) {
+  if (scoring == SD_SCORING_PYDOCK) return pydock_kernel_ptr(precision, false, spill);
   switch (precision) {
-    case SD_PREC_FP64_REF: return (const void*)dfire_score_kernel<SD_PREC_FP64_REF>;
-    case SD_PREC_FP64: return (const void*)dfire_score_kernel<SD_PREC_FP64>;
-    default: return mixed_variant(variant).fn;
+    case SD_PREC_FP64_REF:
+      return spill ? (const void*)dfire_score_kernel<SD_PREC_FP64_REF, true>
+                   : (const void*)dfire_score_kernel<SD_PREC_FP64_REF, false>;
+    case SD_PREC_FP64:
+      return spill ? (const void*)dfire_score_kernel<SD_PREC_FP64, true>
+                   : (const void*)dfire_score_kernel<SD_PREC_FP64, false>;
+    default: return spill ? kMixedSpill.fn : mixed_variant(variant).fn;
   }
 }
 
 int score_launch(const ScoreLaunch& L, int precision, int scoring, int grid, int threads, size_t smem,
-                 cudaStream_t st, int variant) {
-  if (scoring == SD_SCORING_PYDOCK) return pydock_launch(L, precision, false, nullptr, grid, smem, st);
-  switch (precision) {
-    case SD_PREC_FP64_REF: dfire_score_kernel<SD_PREC_FP64_REF><<<grid, threads, smem, st>>>(L); break;
-    case SD_PREC_FP64: dfire_score_kernel<SD_PREC_FP64><<<grid, threads, smem, st>>>(L); break;
-    default: {
-      const MixedVariant& v = mixed_variant(variant);
-      void* args[] = {(void*)&L};
-      if (cudaLaunchKernel(v.fn, dim3(grid), dim3(v.warps * 32), args, smem, st) != cudaSuccess) return SD_ERR_CUDA;
-      break;
-    }
-  }
+                 cudaStream_t st, int variant, bool spill) {
+  if (scoring == SD_SCORING_PYDOCK) return pydock_launch(L, precision, false, nullptr, grid, smem, st, spill);
+  const void* fn = score_kernel_ptr(precision, scoring, variant, spill);
+  const int nthreads = precision == SD_PREC_MIXED ? (spill ? kMixedSpill.warps : mixed_variant(variant).warps) * 32
+                                                  : threads;
+  ScoreLaunch l = L;
+  void* args[] = {(void*)&l};
+  if (cudaLaunchKernel(fn, dim3(grid), dim3(nthreads), args, spill ? 0 : smem, st) != cudaSuccess) return SD_ERR_CUDA;
   return cudaGetLastError() == cudaSuccess ? SD_OK : SD_ERR_CUDA;
 }
 

@@ -82,12 +82,15 @@ struct __align__(16) RingBufs {
 }  // namespace
 
 // Variants differ only in warps per CTA and resident CTAs per SM: a tile is always processed by
-// one warp in the same way, so they give identical energies.
-template <int kWarps, int kMinBlocks>
+// one warp in the same way, so they give identical energies.  kSpill: the per-pose arrays (tile
+// sums, transformed ligand, chunk spheres, tile lists) live in this CTA's slice of the global
+// scratch L.spill, for complexes too large for shared memory; the arithmetic is the same.
+template <int kWarps, int kMinBlocks, bool kSpill>
 __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_kernel(ScoreLaunch L) {
   constexpr int kG = 64;  // entries per stage-2 round, two per lane
   constexpr int kSortMax = 512;        // near tiles ordered largest-first up to this many
-  extern __shared__ __align__(16) unsigned char smem[];
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  unsigned char* const smem = kSpill ? L.spill + (size_t)blockIdx.x * L.spill_stride : smem_dyn;
   __shared__ RingBufs wb[kWarps];
   __shared__ double sh_pose[7 + 2 * SD_MAX_MODES];
   __shared__ double sh_q[4], sh_qi[4];
