@@ -126,6 +126,7 @@ struct sd_ctx {
   StepCtl* d_ctl_scratch = nullptr;
   int* d_work[2] = {nullptr, nullptr};
   int* d_swarm_map = nullptr;
+  double* d_pos_prev = nullptr;  // swarms over SD_MAX_G glowworms: pre-move pose copies
   int total_glowworms = 0;
   int total_swarms = 0;
   int max_nr = 0, max_nl = 0, max_G = 0;
@@ -184,8 +185,8 @@ int check_desc(const sd_complex_desc& d, int scoring) {
   if (d.n_rec <= 0 || d.n_lig <= 0) return fail(SD_ERR_ARG, "complex: empty receptor or ligand");
   if (d.n_rec > SD_MAX_REC) return fail(SD_ERR_ARG, "complex: receptor has more than 4,194,304 atoms");
   if (d.n_lig > SD_MAX_LIG) return fail(SD_ERR_ARG, "complex: ligand has more than 65,504 atoms");
-  if (d.n_swarms <= 0 || d.n_glowworms <= 0 || d.n_glowworms > SD_MAX_G)
-    return fail(SD_ERR_ARG, "complex: swarms must be > 0 and glowworms in 1..1024");
+  if (d.n_swarms <= 0 || d.n_glowworms <= 0 || d.n_glowworms > SD_MAX_GLOWWORMS)
+    return fail(SD_ERR_ARG, "complex: swarms must be > 0 and glowworms in 1..6144");
   if ((long long)d.n_swarms * d.n_glowworms >= (1 << 24))
     return fail(SD_ERR_ARG, "complex: more than 2^24 glowworms");
   if (d.n_modes_rec < 0 || d.n_modes_rec > SD_MAX_MODES || d.n_modes_lig < 0 || d.n_modes_lig > SD_MAX_MODES)
@@ -645,8 +646,9 @@ int enqueue_step(sd_ctx* c, int precision, int grid, size_t sm) {
   G.p.step_r = c->params.rotation_step;
   G.p.step_nm = c->params.nmodes_step;
   G.p.max_neighbors = c->params.max_neighbors;
+  G.pos_prev = c->d_pos_prev;
   const int threads = (c->max_G + 31) / 32 * 32;
-  if ((rc = gso_launch(G, threads, c->stream)))
+  if ((rc = c->max_G > SD_MAX_G ? gso_launch_large(G, c->max_G, c->stream) : gso_launch(G, threads, c->stream)))
     return fail(rc, std::string("GSO kernel launch: ") + cudaGetErrorString(cudaGetLastError()));
   return SD_OK;
 }
@@ -789,6 +791,12 @@ int sd_ctx_create(const sd_complex_desc* complexes, int n_complexes, const sd_ta
   for (int p = 0; p < 2; ++p)
     if ((rc = cu(cudaMalloc(&c->d_work[p], sizeof(int) * std::max(1, c->total_glowworms)), "cudaMalloc"))) return bail(rc);
   if ((rc = cu(cudaMalloc(&c->d_swarm_map, sizeof(int) * c->total_swarms), "cudaMalloc"))) return bail(rc);
+  if (c->max_G > SD_MAX_G) {
+    if ((rc = cu(cudaMalloc(&c->d_pos_prev, sizeof(double) * SD_POSE_LEN(SD_MAX_MODES, SD_MAX_MODES) *
+                                               (size_t)c->total_glowworms), "cudaMalloc")))
+      return bail(rc);
+    if ((rc = gso_prepare_large())) return bail(fail(rc, "large-swarm GSO kernel: shared memory attribute"));
+  }
   {
     std::vector<double> t64(SD_TABLE_SIZE + 32, 0.0);
     for (int i = 0; i < SD_TABLE_SIZE; ++i) {
@@ -836,7 +844,7 @@ int sd_ctx_destroy(sd_ctx* c) {
   for (auto& h : c->cx)
     for (void* p : h.owned) cudaFree(p);
   void* ps[] = {c->d_cplx, c->d_cplx_scratch, c->d_table64, c->d_tablek, c->d_lj_eps, c->d_lj_sigma, c->d_ctl,
-                c->d_ctl_scratch, c->d_work[0], c->d_work[1], c->d_swarm_map, c->s_pose.p, c->s_score.p,
+                c->d_ctl_scratch, c->d_work[0], c->d_work[1], c->d_swarm_map, c->d_pos_prev, c->s_pose.p, c->s_score.p,
                 c->s_ref.p, c->s_energy.p, c->s_work.p, c->s_grad.p, c->s_bins.p, c->s_spill.p};
   for (void* p : ps)
     if (p) cudaFree(p);

@@ -75,6 +75,84 @@ __device__ __forceinline__ void slerp_dev(double* self, double* other, double st
   }
 }
 
+// Neighbours of glowworm g (luciferin shL[G] and reference points shR[G][3] of its swarm in shared
+// memory; vision range vr) in ascending n (prepare_gso_tasks.cc:615-640), their probability total
+// (:1476-1484) and the first whose cumulative probability reaches the draw *u (:1441-1450).
+// Returns the choice (g itself without neighbours) and the count in nn; counts the draws <= 0 with
+// neighbours (the reference reads neighbors[-1]; the first is taken) and the cumulative shortfalls
+// (the last is taken).
+__device__ __forceinline__ int choose_neighbour(const double* shL, const double* shR, int G, int g, double Lg,
+                                                double vr, const double* u_ptr, int& nn,
+                                                unsigned long long* uzero, unsigned long long* shortfall) {
+  const double cx = shR[g * 3], cy = shR[g * 3 + 1], cz = shR[g * 3 + 2];
+  const double sq = vr * vr;
+  double total = 0;
+  nn = 0;
+  for (int n = 0; n < G; ++n) {
+    const double Ln = shL[n];
+    if (n != g && Lg < Ln) {
+      const double dx = cx - shR[n * 3], dy = cy - shR[n * 3 + 1], dz = cz - shR[n * 3 + 2];
+      double distance = 0;
+      distance += dx * dx;
+      distance += dy * dy;
+      distance += dz * dz;
+      if (distance < sq) {
+        ++nn;
+        total += Ln - Lg;
+      }
+    }
+  }
+  if (nn == 0) return g;
+  const double u = *u_ptr;
+  double sum = 0.0;
+  int picked = -1, last = -1;
+  if (!(sum < u)) atomicAdd(uzero, 1ull);
+  for (int n = 0; n < G && picked < 0; ++n) {
+    const double Ln = shL[n];
+    if (n != g && Lg < Ln) {
+      const double dx = cx - shR[n * 3], dy = cy - shR[n * 3 + 1], dz = cz - shR[n * 3 + 2];
+      double distance = 0;
+      distance += dx * dx;
+      distance += dy * dy;
+      distance += dz * dz;
+      if (distance < sq) {
+        last = n;
+        if (!(sum < u)) {
+          picked = n;  // only reached when u <= 0
+        } else {
+          sum += (Ln - Lg) / total;
+          if (!(sum < u)) picked = n;
+        }
+      }
+    }
+  }
+  if (picked < 0) {
+    picked = last;
+    atomicAdd(shortfall, 1ull);
+  }
+  return picked;
+}
+
+// Movement of one glowworm towards the chosen neighbour's pose mv (prepare_gso_tasks.cc:772-794):
+// translation by step_t along the direction, slerp of the quaternion, receptor and ligand extents.
+__device__ __forceinline__ void move_towards(double* cur, double* mv, int nmr, int nml, const GsoParamsDev& P) {
+  double delta[3], n = 0;
+  for (int d = 0; d < 3; ++d) {
+    delta[d] = mv[d] - cur[d];
+    n += (delta[d] * delta[d]);
+  }
+  n = sqrt(n);
+  if (n >= 1e-8) {
+    for (int d = 0; d < 3; ++d) {
+      delta[d] *= (P.step_t / n);
+      cur[d] += delta[d];
+    }
+  }
+  slerp_dev(cur + 3, mv + 3, P.step_r);
+  move_extent_dev(cur + 7, mv + 7, nmr, P.step_nm);
+  move_extent_dev(cur + 7 + nmr, mv + 7 + nmr, nml, P.step_nm);
+}
+
 __global__ void __launch_bounds__(SD_MAX_G) gso_kernel(GsoLaunch L) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int sh_base, sh_last;
@@ -107,60 +185,10 @@ __global__ void __launch_bounds__(SD_MAX_G) gso_kernel(GsoLaunch L) {
   }
   __syncthreads();
   int sel = g, nn = 0;
-  if (live) {
-    const double cx = shR[g * 3], cy = shR[g * 3 + 1], cz = shR[g * 3 + 2];
-    const double vr = C.vision[k];
-    const double sq = vr * vr;
-    // neighbours in ascending n (:615-640) and the probability total (:1476-1484)
-    double total = 0;
-    for (int n = 0; n < G; ++n) {
-      const double Ln = shL[n];
-      if (n != g && Lg < Ln) {
-        const double dx = cx - shR[n * 3], dy = cy - shR[n * 3 + 1], dz = cz - shR[n * 3 + 2];
-        double distance = 0;
-        distance += dx * dx;
-        distance += dy * dy;
-        distance += dz * dz;
-        if (distance < sq) {
-          ++nn;
-          total += Ln - Lg;
-        }
-      }
-    }
-    if (nn > 0) {
-      // selection (:1441-1450): first neighbour whose cumulative probability reaches u
-      const double u = C.draws[(size_t)s * C.draw_steps * G + (size_t)C.draw_cursor * G + g];
-      double sum = 0.0;
-      int picked = -1, last = -1;
-      if (!(sum < u)) {
-        atomicAdd(&sh_uzero, 1ull);  // u <= 0: reference reads neighbors[-1]; take the first
-      }
-      for (int n = 0; n < G && picked < 0; ++n) {
-        const double Ln = shL[n];
-        if (n != g && Lg < Ln) {
-          const double dx = cx - shR[n * 3], dy = cy - shR[n * 3 + 1], dz = cz - shR[n * 3 + 2];
-          double distance = 0;
-          distance += dx * dx;
-          distance += dy * dy;
-          distance += dz * dz;
-          if (distance < sq) {
-            last = n;
-            if (!(sum < u)) {
-              picked = n;  // only reached when u <= 0
-            } else {
-              sum += (Ln - Lg) / total;
-              if (!(sum < u)) picked = n;
-            }
-          }
-        }
-      }
-      if (picked < 0) {
-        picked = last;
-        atomicAdd(&sh_short, 1ull);  // cumulative probability short of u
-      }
-      sel = picked;
-    }
-  }
+  if (live)
+    sel = choose_neighbour(shL, shR, G, g, Lg, C.vision[k],
+                           C.draws + (size_t)s * C.draw_steps * G + (size_t)C.draw_cursor * G + g, nn, &sh_uzero,
+                           &sh_short);
   // copy of the chosen neighbour's pre-move position (:689-693)
   double mv[7 + 2 * SD_MAX_MODES], cur[7 + 2 * SD_MAX_MODES];
   if (live) {
@@ -179,22 +207,7 @@ __global__ void __launch_bounds__(SD_MAX_G) gso_kernel(GsoLaunch L) {
     C.nnei[k] = nn;
     C.select[k] = sel;
     if (moved) {
-      // translation (:772-786)
-      double delta[3], n = 0;
-      for (int d = 0; d < 3; ++d) {
-        delta[d] = mv[d] - cur[d];
-        n += (delta[d] * delta[d]);
-      }
-      n = sqrt(n);
-      if (n >= 1e-8) {
-        for (int d = 0; d < 3; ++d) {
-          delta[d] *= (P.step_t / n);
-          cur[d] += delta[d];
-        }
-      }
-      slerp_dev(cur + 3, mv + 3, P.step_r);
-      move_extent_dev(cur + 7, mv + 7, C.nmr, P.step_nm);
-      move_extent_dev(cur + 7 + C.nmr, mv + 7 + C.nmr, C.nml, P.step_nm);
+      move_towards(cur, mv, C.nmr, C.nml, P);
       double* own = C.pos + k * pl;
       for (int i = 0; i < pl; ++i) own[i] = cur[i];
     }
@@ -251,10 +264,138 @@ __global__ void __launch_bounds__(SD_MAX_G) gso_kernel(GsoLaunch L) {
   }
 }
 
+// Swarms of more than SD_MAX_G glowworms (more than one CTA's threads): the same update with each
+// thread taking glowworms tid, tid + blockDim.x, ...  A thread can no longer hold the chosen
+// neighbours' pre-move poses of all its glowworms across a barrier, so every pose is first copied to
+// L.pos_prev (one row of SD_POSE_LEN(10, 10) doubles per glowworm of the context) and the moves read
+// the copies.  Moved glowworms are appended to the next work list one CTA-wide chunk at a time.
+__global__ void __launch_bounds__(SD_MAX_G) gso_kernel_large(GsoLaunch L) {
+  constexpr int kRow = SD_POSE_LEN(SD_MAX_MODES, SD_MAX_MODES);
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int sh_base, sh_last;
+  __shared__ unsigned long long sh_uzero, sh_short;
+  __shared__ int sh_wcount[SD_MAX_G / 32], sh_woff[SD_MAX_G / 32];
+  const int sw_packed = L.swarm_map[blockIdx.x];
+  const int ci = wi_complex(sw_packed), s = wi_local(sw_packed);
+  DevComplex& C = L.cplx[ci];
+  const int G = C.G, pl = C.pl, tid = threadIdx.x, B = blockDim.x;
+  double* shL = reinterpret_cast<double*>(smem);  // [G]
+  double* shR = shL + G;                          // [G][3]
+  StepCtl* ctl = L.ctl;
+  const int parity = ctl->parity;
+  const GsoParamsDev P = L.p;
+  double* prev = L.pos_prev + ((size_t)C.gbase + (size_t)s * G) * kRow;
+  if (tid == 0) {
+    sh_uzero = 0;
+    sh_short = 0;
+  }
+  // luciferin (prepare_gso_tasks.cc:558), staging, pre-move copies
+  for (int g = tid; g < G; g += B) {
+    const size_t k = (size_t)s * G + g;
+    const double Lg = (1.0 - P.rho) * C.luciferin[k] + P.gamma * C.scoring[k];
+    C.luciferin[k] = Lg;
+    C.step[k] += 1;
+    shL[g] = Lg;
+    shR[g * 3] = C.ref[k * 3];
+    shR[g * 3 + 1] = C.ref[k * 3 + 1];
+    shR[g * 3 + 2] = C.ref[k * 3 + 2];
+    for (int i = 0; i < pl; ++i) prev[(size_t)g * kRow + i] = C.pos[k * pl + i];
+  }
+  __syncthreads();
+  unsigned moved_bits = 0;  // bit c: glowworm c * B + tid moved
+  for (int g = tid, c = 0; g < G; g += B, ++c) {
+    const size_t k = (size_t)s * G + g;
+    int nn = 0;
+    const int sel = choose_neighbour(shL, shR, G, g, shL[g], C.vision[k],
+                                     C.draws + (size_t)s * C.draw_steps * G + (size_t)C.draw_cursor * G + g, nn,
+                                     &sh_uzero, &sh_short);
+    const bool moved = sel != g;
+    C.moved[k] = moved ? 1 : 0;
+    C.nnei[k] = nn;
+    C.select[k] = sel;
+    if (moved) {
+      double mv[kRow], cur[kRow];
+      for (int i = 0; i < pl; ++i) {
+        mv[i] = prev[(size_t)sel * kRow + i];
+        cur[i] = prev[(size_t)g * kRow + i];
+      }
+      move_towards(cur, mv, C.nmr, C.nml, P);
+      for (int i = 0; i < pl; ++i) C.pos[k * pl + i] = cur[i];
+      moved_bits |= 1u << c;
+    }
+    // vision range (:806-808)
+    double vr = C.vision[k] + P.beta * (P.max_neighbors - nn);
+    if (vr < 0.0) vr = 0;
+    if (vr > P.max_vision) vr = P.max_vision;
+    C.vision[k] = vr;
+  }
+  // next work list, chunk by chunk, in glowworm order within a chunk
+  const int lane = tid & 31, wid = tid >> 5, nw = B >> 5;
+  for (int c = 0; c * B < G; ++c) {
+    const bool moved = (moved_bits >> c) & 1u;
+    const unsigned bal = __ballot_sync(0xffffffffu, moved);
+    if (lane == 0) sh_wcount[wid] = __popc(bal);
+    __syncthreads();
+    if (tid == 0) {
+      int acc = 0;
+      for (int w = 0; w < nw; ++w) {
+        sh_woff[w] = acc;
+        acc += sh_wcount[w];
+      }
+      sh_base = acc ? atomicAdd(&ctl->count[parity ^ 1], acc) : 0;
+    }
+    __syncthreads();
+    if (moved) {
+      const int pos_in = sh_base + sh_woff[wid] + __popc(bal & ((1u << lane) - 1u));
+      L.work[parity ^ 1][pos_in] = wi_pack(ci, s * G + c * B + tid);
+    }
+    __syncthreads();
+  }
+  // last block advances the step
+  if (tid == 0) {
+    if (sh_uzero) atomicAdd(&ctl->stats[ST_UZERO], sh_uzero);
+    if (sh_short) atomicAdd(&ctl->stats[ST_SHORT], sh_short);
+    __threadfence();
+    const int done = atomicAdd(&ctl->done_blocks, 1);
+    sh_last = done == L.nswarms_total - 1;
+  }
+  __syncthreads();
+  if (sh_last && tid == 0) {
+    __threadfence();
+    ctl->count[parity] = 0;
+    ctl->grab[parity] = 0;
+    ctl->grab[parity ^ 1] = 0;
+    ctl->parity = parity ^ 1;
+    ctl->done_blocks = 0;
+    ctl->step += 1;
+    ctl->stats[ST_STEPS] += 1;
+    __threadfence();
+  }
+  if (sh_last && tid < L.ncplx) {
+    __threadfence();
+    L.cplx[tid].draw_cursor += 1;
+  }
+}
+
 int gso_launch(const GsoLaunch& L, int threads, cudaStream_t st) {
   // shared: luciferin + reference points of the swarm's glowworms
   const size_t smem = (size_t)SD_MAX_G * 4 * sizeof(double);
   gso_kernel<<<L.nswarms_total, threads, smem, st>>>(L);
+  return cudaGetLastError() == cudaSuccess ? SD_OK : SD_ERR_CUDA;
+}
+
+// once per context that has such swarms, before any capture: the large kernel's shared memory
+int gso_prepare_large() {
+  return cudaFuncSetAttribute((const void*)gso_kernel_large, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)((size_t)SD_MAX_GLOWWORMS * 4 * sizeof(double))) == cudaSuccess
+             ? SD_OK
+             : SD_ERR_CUDA;
+}
+
+int gso_launch_large(const GsoLaunch& L, int max_g, cudaStream_t st) {
+  // shared: luciferin + reference points of the swarm's glowworms
+  const size_t smem = (size_t)max_g * 4 * sizeof(double);
+  gso_kernel_large<<<L.nswarms_total, SD_MAX_G, smem, st>>>(L);
   return cudaGetLastError() == cudaSuccess ? SD_OK : SD_ERR_CUDA;
 }
 

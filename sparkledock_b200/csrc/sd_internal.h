@@ -23,7 +23,8 @@
 #define SD_TILE 32              /* receptor atoms per tile (one warp lane each) */
 #define SD_MAX_LIG 65504        /* ligand atoms: the mixed scorer's 16-bit ligand slot indices */
 #define SD_MAX_REC (1 << 22)    /* receptor atoms */
-#define SD_MAX_G 1024           /* glowworms per swarm (one thread each) */
+#define SD_MAX_G 1024           /* glowworms per swarm with one thread each (one CTA per swarm) */
+#define SD_MAX_GLOWWORMS 6144   /* glowworms per swarm: luciferin + reference points in shared memory */
 #define SD_CULL_MARGIN 0.05f    /* A, covers FP32 rounding of the conservative culling tests */
 #define SD_MAX_VARIANTS 16      /* compiled variants of the mixed DFIRE kernel (autotuner) */
 #define SD_NOALLOC_MAX_POSES 65536           /* poses per sd_score_poses_noalloc call */
@@ -152,6 +153,7 @@ struct GsoLaunch {
   int nswarms_total;
   int ncplx;               // <= 32 (the last CTA's first warp advances their draw cursors)
   GsoParamsDev p;
+  double* pos_prev;        // swarms over SD_MAX_G glowworms: pre-move pose copies [glowworms][27]
 };
 
 // kernel launchers (sd_score.cu, sd_gso.cu)
@@ -166,6 +168,8 @@ int mixed_variant_count();
 int mixed_variant_warps(int v);
 int mixed_variant_min_blocks(int v);
 int gso_launch(const GsoLaunch& L, int threads, cudaStream_t st);
+int gso_launch_large(const GsoLaunch& L, int max_g, cudaStream_t st);
+int gso_prepare_large();
 int bins_launch(const DevComplex* cplx, int c, const double* d_pose, int precision, int* d_bins, int nr, int nl,
                 int* d_fallback, cudaStream_t st);
 size_t pydock_smem_bytes(int precision, bool grad, int max_nl, int max_nr);

@@ -89,3 +89,34 @@ def test_noalloc_needs_a_sized_scratch_for_large_complexes(tables):
         sc, en = dk.score_poses(0, poses, sd.SD_PREC_MIXED)  # sizes the context's scratch
         assert call() == 0, _abi.lib().sd_last_error()
         assert np.array_equal(d_sc.cpu().numpy(), sc) and np.array_equal(d_en.cpu().numpy(), en)
+
+
+@pytest.mark.parametrize("precision", [sd.SD_PREC_FP64, sd.SD_PREC_MIXED], ids=["fp64", "mixed"])
+def test_swarms_larger_than_a_cta(precision, tables):
+    """Swarms of more than 1,024 glowworms (one CTA's threads) next to an ordinary one in the same
+    context: every state field bit-identical to the oracle every step (FP64), or when the oracle's
+    update is fed the GPU's scores (mixed, step-locked)."""
+    cxs = [sd.SyntheticComplex(300, 200, 2, 1500, 10, 10, seed=34), sd.SyntheticComplex(400, 150, 1, 200, 10, 10,
+                                                                                         seed=35)]
+    steps = 3
+    Us = [sd.gso_draws(6 + i, c.n_swarms, steps, c.n_glowworms) for i, c in enumerate(cxs)]
+    osyss = [OracleSystem(c, tables) for c in cxs]
+    sts = [OracleState(c.n_swarms, c.n_glowworms, c.pose_len, c.poses) for c in cxs]
+    with sd.Docking(cxs, tables, precision=precision) as dk:
+        for i, c in enumerate(cxs):
+            dk.init_state(i, c.poses)
+            dk.set_draws(i, Us[i])
+        for t in range(steps):
+            dk.step(1)
+            for i, c in enumerate(cxs):
+                g = dk.get_state(i)
+                if precision == sd.SD_PREC_FP64:
+                    oracle_step(osyss[i], sts[i], Us[i][:, t, :])
+                else:
+                    free = sts[i].copy()
+                    rescored = (free.moved == 1) | (free.step == 0)
+                    oracle_step(osyss[i], free, Us[i][:, t, :])
+                    assert rel_err(g.scoring[rescored], free.scoring[rescored]).max() <= 1e-5
+                    oracle_step(osyss[i], sts[i], Us[i][:, t, :], score_override=g.scoring)
+                for f, o in FIELDS + (("moved", "moved"), ("step", "step")):
+                    assert np.array_equal(getattr(g, f), getattr(sts[i], o)), f"complex {i} step {t}: {f}"
