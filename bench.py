@@ -143,6 +143,7 @@ def run_gpu(cfg, prec_name, steps, warmup, device, flush, seed=0, per_step=False
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
     scored_steps = []
+    pair_steps = []
     energy_err = []
     with torch.cuda.stream(stream):
         for k in range(steps):
@@ -154,7 +155,9 @@ def run_gpu(cfg, prec_name, steps, warmup, device, flush, seed=0, per_step=False
             dk.step(1, sync=False)
             ends[k].record(stream)
             if per_step:  # synchronises between steps (outside the timed events)
-                scored_steps.append(dk.stats()["scored_poses"])
+                st = dk.stats()
+                scored_steps.append(st["scored_poses"])
+                pair_steps.append(st["pairs_in_cutoff"])
             if check:
                 energy_err.append(step_energy_error(dk, cxs, before, k))
     torch.cuda.synchronize(device)
@@ -164,6 +167,8 @@ def run_gpu(cfg, prec_name, steps, warmup, device, flush, seed=0, per_step=False
            "pairs": s1["pairs_in_cutoff"] - s0["pairs_in_cutoff"],
            "tuning": dk.tuning(),
            "per_step": [b - a for a, b in zip([s0["scored_poses"]] + scored_steps, scored_steps)] if per_step else None,
+           "per_step_pairs": ([b - a for a, b in zip([s0["pairs_in_cutoff"]] + pair_steps, pair_steps)]
+                              if per_step else None),
            "energy_err": energy_err}
     return out
 
@@ -679,7 +684,8 @@ def main():
         "c1": c1,
         "final_clustering": clustering,
         "setup": setup,
-        **({"per_step": {"scored_poses": run["per_step"], "ms": run["ms"]}} if args.per_step else {}),
+        **({"per_step": {"scored_poses": run["per_step"], "pairs_in_cutoff": run["per_step_pairs"], "ms": run["ms"]}}
+           if args.per_step else {}),
         "edge_counts": {k: stats[k] for k in ("pairs_fallback", "edge_d2_zero", "edge_d2_cutoff", "edge_u_zero",
                                               "edge_shortfall")},
     }
