@@ -177,7 +177,10 @@ __global__ void __launch_bounds__(kFp64Threads) dfire_score_kernel(ScoreLaunch L
         if (keep) {
           const int at = atomicAdd(&sh_ntile, 1);
           tlist[at] = k;
-          tdist[at] = cx * cx + cy * cy + cz * cz;
+          // a NaN distance (non-finite pose) ranks last: the ranking below must stay a strict total
+          // order, or tord would not be a permutation of the kept tiles
+          const float dd = cx * cx + cy * cy + cz * cz;
+          tdist[at] = dd == dd ? dd : 3.0e38f;
         }
       } else {
         tlist[atomicAdd(&sh_ntile, 1)] = k;

@@ -215,7 +215,10 @@ __global__ void __launch_bounds__(kWarps * 32, kMinBlocks) dfire_score_mixed_ker
         const int at = atomicAdd(&sh_ntile, 1);
         const float ex = cx - sh_gc[0], ey = cy - sh_gc[1], ez = cz - sh_gc[2];
         tlist[at] = k;
-        tdist[at] = ex * ex + ey * ey + ez * ez;
+        // a NaN distance (non-finite quaternion) ranks last: the ranking below must stay a strict
+        // total order, or tord would not be a permutation of the near tiles
+        const float dd = ex * ex + ey * ey + ez * ez;
+        tdist[at] = dd == dd ? dd : 3.0e38f;
       }
     }
     __syncthreads();

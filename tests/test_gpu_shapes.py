@@ -9,7 +9,9 @@ seeds), with a few swarms so that the CPU oracle finishes in seconds.  Bars:
     pinned bit-identical to the oracle) on every pose of the sample, and mixed bins identical;
   * the single complex's GSO update bit-identical to the oracle's for 3 steps when fed the GPU's
     mixed scores (step-locked), and a batched FP64 step of all eight complexes bit-identical;
-  * the adjoint (FP32) within 1e-4 of the FP64 GPU gradient, which is within 1e-10 of the oracle's.
+  * the adjoint (FP32) within 1e-4 of the FP64 GPU gradient, which is within 1e-10 of the oracle's;
+    its FP32 energy within the same 1e-4 (the FP32 pair terms of ~60k pairs per pose: 4.3e-5 was
+    measured at this size, where the DFIRE scorer's FP64 table sums reach 1e-13).
 """
 import numpy as np
 import pytest
@@ -122,7 +124,7 @@ def test_adjoint_shape(tables):
         e32, g32 = dk.pydock_grad(0, poses, sd.SD_PREC_MIXED)
     scale = np.maximum(np.abs(g64).max(axis=1), 1.0)
     assert (np.abs(g32 - g64).max(axis=1) / scale).max() <= 1e-4
-    assert rel_err(e32, e64).max() <= MIXED_TOL
+    assert rel_err(e32, e64).max() <= 1e-4
     osys = OracleSystem(cx, tables, scoring=1)
     for k in range(4):
         ref = oracle_grad(osys, poses[k], ng)

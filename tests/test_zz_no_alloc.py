@@ -2,9 +2,10 @@
 memory while they score (graph capture, or a framework that owns all device memory).  It is
 checked through the C ABI against the allocating entry point sd_score_poses on the same poses,
 for two calls in a row (the second with other poses, so a stale scratch would show), in every
-precision and with both scoring functions: bit-identical scores and energies (the mixed kernel's
-summation order is fixed, so it too is reproducible to the bit), ligand reference points
-bit-identical to the oracle's.  A non-finite pose is reported with sync; sync is refused while
+precision and with both scoring functions: DFIRE scores and energies bit-identical (the mixed
+kernel's summation order is fixed, so it too is reproducible to the bit); pyDock ones within
+1e-10 (FP64) and 1e-5 (FP32) relative, since that kernel's per-lane sums follow the dynamic tile
+order; ligand reference points bit-identical to the oracle's.  A non-finite pose is reported with sync; sync is refused while
 the stream is being captured.  This file is collected last on purpose."""
 import ctypes as C
 
@@ -53,7 +54,12 @@ def test_noalloc_matches_allocating_entry_point(scoring, tables):
                 ref_sc, ref_en = dk.score_poses(0, poses, prec)
                 rc, sc, en, refp = noalloc(dk, poses, prec)
                 assert rc == 0, _abi.lib().sd_last_error()
-                assert np.array_equal(sc, ref_sc) and np.array_equal(en, ref_en), f"precision {prec} call {call}"
+                if scoring == sd.SD_SCORING_DFIRE:
+                    assert np.array_equal(sc, ref_sc) and np.array_equal(en, ref_en), f"precision {prec} call {call}"
+                else:
+                    tol = 1e-5 if prec == sd.SD_PREC_MIXED else 1e-10
+                    err = np.abs(en - ref_en) / np.maximum(np.abs(ref_en), 1.0)
+                    assert err.max() <= tol and np.array_equal(sc, -en), f"precision {prec} call {call}"
                 assert np.array_equal(refp, oracle_ref_points(cx, tables, poses)), f"precision {prec} call {call}"
 
 
