@@ -212,8 +212,13 @@ int sd_write_pose_pdb(const char* path, const sd_structure* receptor, const doub
 int sd_anm(const sd_structure* s, int n_modes, double rmsd, int n_swarms, int n_glowworms, int device,
            double* modes_out, double* xyz_out, double* eigvals_out);
 /* Khachiyan minimum-volume enclosing ellipsoid centre of n points (tolerance 0.01), the ligand
- * reference point of minimum_volume_ellipsoid (source/dock/src/prepare_gso_tasks.cc:106-267). */
+ * reference point of minimum_volume_ellipsoid (source/dock/src/prepare_gso_tasks.cc:106-267):
+ * its operation order, including that of the Eigen 4x4 inverse it calls, so the centre is
+ * bit-identical to the reference's (single-threaded) result; O(n) per iteration. */
 int sd_reference_point(const double* xyz, int n, double* center);
+/* The same centre computed on `device` (one CTA; the reference's summation orders kept), bit-identical
+ * to sd_reference_point. */
+int sd_reference_point_device(int device, const double* xyz, int n, double* center);
 /* Seeded starting poses [n_swarms][n_glowworms][pose_len] around a receptor centred at the
  * origin, for synthetic complexes (no residues to place swarms on): swarm centres at uniform
  * directions on a shell 10 A outside its bounding sphere, each glowworm at its centre plus

@@ -94,6 +94,7 @@ SIGNATURES = {
     "sd_mixed_variant_count": (C.c_int, []),
     "sd_structure_load": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]),
     "sd_reference_point": (C.c_int, [_dp, C.c_int, _dp]),
+    "sd_reference_point_device": (C.c_int, [C.c_int, _dp, C.c_int, _dp]),
     "sd_anm": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp]),
     "sd_place_swarms": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                   C.c_int, C.c_double, C.c_int, C.c_int, _dp, _dp]),

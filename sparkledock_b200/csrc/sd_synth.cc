@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "sd_internal.h"
+#include "sd_mvee.h"
 
 namespace sd {
 
@@ -139,56 +140,7 @@ void starting_poses(Rng& rs, const double* rec_xyz, int n_rec, int S, int G, int
   }
 }
 
-namespace {
 
-// Inverse of a 4x4 matrix (column-major, a[c*4 + r]) in the operation order of the reference's
-// MatrixXd::inverse() (its vendored Eigen 3.4: PartialPivLU, then solve against the identity):
-//  * LU with partial pivoting, column by column: pivot = first row of largest |a(r,k)|, rows
-//    swapped, the column below divided by the pivot, then a(r,c) -= a(r,k) * a(k,c);
-//  * X = P I (the same row swaps applied to the identity);
-//  * unit-lower solve, top to bottom: X(r,j) -= X(k,j) * L(r,k) for r > k;
-//  * upper solve, bottom to top: X(i,j) *= 1 / U(i,i), then X(r,j) -= X(i,j) * U(r,i) for r < i.
-void inverse4_lu(const double* a, double* x) {
-  double lu[16];
-  for (int k = 0; k < 16; ++k) lu[k] = a[k];
-  int piv[4];
-  for (int k = 0; k < 4; ++k) {
-    int p = k;
-    double best = std::fabs(lu[k * 4 + k]);
-    for (int r = k + 1; r < 4; ++r)
-      if (std::fabs(lu[k * 4 + r]) > best) {
-        best = std::fabs(lu[k * 4 + r]);
-        p = r;
-      }
-    piv[k] = p;
-    if (best != 0.0) {
-      if (p != k)
-        for (int c = 0; c < 4; ++c) std::swap(lu[c * 4 + k], lu[c * 4 + p]);
-      for (int r = k + 1; r < 4; ++r) lu[k * 4 + r] /= lu[k * 4 + k];
-    }
-    for (int c = k + 1; c < 4; ++c)
-      for (int r = k + 1; r < 4; ++r) lu[c * 4 + r] -= lu[c * 4 + k] * lu[k * 4 + r];
-  }
-  for (int k = 0; k < 16; ++k) x[k] = (k % 5 == 0) ? 1.0 : 0.0;
-  for (int k = 0; k < 4; ++k)
-    if (piv[k] != k)
-      for (int c = 0; c < 4; ++c) std::swap(x[c * 4 + k], x[c * 4 + piv[k]]);
-  for (int k = 0; k < 4; ++k)
-    for (int j = 0; j < 4; ++j) {
-      const double b = x[j * 4 + k];
-      for (int r = k + 1; r < 4; ++r) x[j * 4 + r] -= b * lu[k * 4 + r];
-    }
-  for (int i = 3; i >= 0; --i) {
-    const double inv = 1.0 / lu[i * 4 + i];
-    for (int j = 0; j < 4; ++j) {
-      x[j * 4 + i] *= inv;
-      const double b = x[j * 4 + i];
-      for (int r = 0; r < i; ++r) x[j * 4 + r] -= b * lu[i * 4 + r];
-    }
-  }
-}
-
-}  // namespace
 
 // Khachiyan's minimum-volume enclosing ellipsoid centre with tolerance tol, in the operation
 // order of the reference's minimum_volume_ellipsoid (prepare_gso_tasks.cc:106-267, with its
@@ -219,7 +171,7 @@ void mvee_center(const double* p, int n, double tol, double* center) {
         V[a * 4 + b] = sum;
       }
     double X[16];
-    inverse4_lu(V, X);
+    sd_inverse4_lu(V, X);
     double mx = 0.0;
     int j = 0;
     for (int i = 0; i < n; ++i) {
