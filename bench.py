@@ -58,6 +58,11 @@ L2_FLUSH_BYTES = 256 << 20
 # reference point out), as summarised with the scorer's launch list under profiles/
 DRAM_BYTES_PER_LAUNCH = 9.52e6
 DRAM_BYTES_PER_SCORED_POSE = 144.0
+# warp-instructions the mixed scorer issues per receptor-ligand pair inside the cutoff, from ncu
+# smsp__inst_executed.sum of one launch (3002 / 1274 atoms, 4,098 poses, 233.9 M pairs in the
+# cutoff), as summarised with its full capture under profiles/; the scorer is issue-bound, so its
+# ceiling is the SMs' issue rate (148 SMs x 4 schedulers x clock) over this count
+WARP_INSTR_PER_PAIR = 5.96
 
 
 def make_complexes(cfg, seed0=100):
@@ -548,6 +553,10 @@ def roofline_of(cfg, name, m, args, peaks, peak_src):
                          DRAM_BYTES_PER_SCORED_POSE * m["value"]) / 1e9 / peaks.get("hbm_gbs", 6650.0),
             "brute_force_equivalent": {"tflops": brute, "frac": brute / fp32_peak,
                                        "work": "8 Nr Nl flops per scored pose"},
+            "issue_bound": {"warp_instructions_per_pair": WARP_INSTR_PER_PAIR,
+                            "ceiling_pairs_per_s": 148 * 4 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / WARP_INSTR_PER_PAIR,
+                            "frac": m["pairs_all"] / t_s /
+                                    (148 * 4 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / WARP_INSTR_PER_PAIR)},
             "per_scored_pose": {"pairs_in_cutoff": stats["pairs_in_cutoff"] / max(1, stats["scored_poses"]),
                                 "pairs_evaluated": stats["pairs_evaluated"] / max(1, stats["scored_poses"]),
                                 "pairs_brute_force": brute_pairs_per_pose(cfg)}}
