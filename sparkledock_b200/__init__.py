@@ -69,13 +69,18 @@ class SyntheticComplex:
         self.pose_len = 7 + n_modes_rec + n_modes_lig
         d = self.desc
 
+        base = self._buf.ctypes.data
+
         def view(ptr, shape, dtype):
+            # a slice of self._buf, so every array keeps the buffer alive after the complex is gone
             n = int(np.prod(shape))
             if n == 0:
                 return np.zeros(shape, dtype)
-            ct = C.c_double if dtype == np.float64 else C.c_int
-            arr = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ct)), shape=(n,))
-            return arr.reshape(shape)
+            item = np.dtype(dtype).itemsize
+            off = C.cast(ptr, C.c_void_p).value - base
+            if off < 0 or off + n * item > self._buf.nbytes or off % item:
+                raise SparkleError(_abi.SD_ERR_ARG, "sd_synth_generate: an array outside its buffer")
+            return self._buf[off:off + n * item].view(dtype).reshape(shape)
 
         self.rec_xyz = view(d.rec_xyz, (n_rec, 3), np.float64)
         self.lig_xyz = view(d.lig_xyz, (n_lig, 3), np.float64)

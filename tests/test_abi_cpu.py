@@ -57,6 +57,18 @@ def test_synthetic_complex_properties():
     assert list(cx.desc.lig_ref_point) == [1.5, -2.0, 3.25] and np.array_equal(cx.lig_ref, [1.5, -2.0, 3.25])
 
 
+def test_synthetic_arrays_outlive_their_complex():
+    """An array taken from a temporary complex keeps the complex's buffer alive."""
+    import gc
+    keep = sd.SyntheticComplex(757, 481, 5, 20, seed=4)
+    xyz, poses = sd.SyntheticComplex(757, 481, 5, 20, seed=4).lig_xyz, sd.SyntheticComplex(757, 481, 5, 20,
+                                                                                            seed=4).poses
+    gc.collect()
+    junk = [np.full(1 << 20, np.nan) for _ in range(8)]  # reuse whatever memory was released
+    assert np.array_equal(xyz, keep.lig_xyz) and np.array_equal(poses, keep.poses)
+    del junk
+
+
 def test_ctx_create_without_gpu_is_a_status_not_a_crash(tables):
     if sd.device_count() > 0:
         return
