@@ -21,6 +21,11 @@
  *
  * Threading: one context is used by one host thread at a time; distinct contexts may be
  * used concurrently.  Each context owns one CUDA stream on its device.
+ *
+ * Devices: every call that touches a GPU makes its device (the context's, or the device
+ * argument) current on the calling thread, as cudaSetDevice does, and leaves it current on
+ * return.  A caller that drives several GPUs from one thread selects its own device again
+ * after a call.
  */
 #ifndef SPARKLE_B200_H
 #define SPARKLE_B200_H
