@@ -536,30 +536,33 @@ def roofline_of(cfg, name, m, args, peaks, peak_src):
     (the reference's formulation of the DFIRE sum).  Time: the timed GSO steps (scorer ~99 %)."""
     stats = m["run"]["stats"]
     t_s = m["t_ms"] / 1e3
-    fp32_peak = 148 * 128 * 2 * (peaks.get("sm_max_mhz", 1965.0) * 1e6) / 1e12
+    mixed = cfg["precision"] == "mixed"
+    lanes = 128 if mixed else 64  # FP32 or FP64 vector lanes per SM
+    vec_peak = 148 * lanes * 2 * (peaks.get("sm_max_mhz", 1965.0) * 1e6) / 1e12
     cut_tflops = 8.0 * m["pairs_all"] / t_s / 1e12
     brute = 8.0 * brute_pairs_per_pose(cfg) * m["scored"] / t_s / 1e12
-    return {"bound": "fp32", "achieved": cut_tflops, "peak": fp32_peak, "unit": "TFLOP/s",
-            "frac": cut_tflops / fp32_peak,
+    out = {"bound": "fp32" if mixed else "fp64", "achieved": cut_tflops, "peak": vec_peak, "unit": "TFLOP/s",
+            "frac": cut_tflops / vec_peak,
             "work": "8 flops per receptor-ligand pair inside the 15 A cutoff (counted by the kernel)",
             "pairs_per_s": m["pairs_all"] / t_s,
             "table_bytes_per_s": 8.0 * m["pairs_all"] / t_s,
             "traffic": DRAM_BYTES_PER_LAUNCH + DRAM_BYTES_PER_SCORED_POSE * m["scored"] / args.steps,
             "traffic_unit": "bytes per launch (DRAM, ncu: fixed + per rescored pose)",
-            "peak_source": "nominal FP32 vector pipe (148 SMs x 128 lanes x 2) at the measured "
-                           f"max SM clock {peaks.get('sm_max_mhz', 1965.0):.0f} MHz "
-                           f"({peak_src} peaks file has no FP32 vector figure)",
+            "peak_source": f"nominal {'FP32' if mixed else 'FP64'} vector pipe (148 SMs x {lanes} lanes x 2) at the "
+                           f"measured max SM clock {peaks.get('sm_max_mhz', 1965.0):.0f} MHz "
+                           f"({peak_src} peaks file has no FP32 or FP64 vector figure)",
             "hbm_frac": (DRAM_BYTES_PER_LAUNCH * args.steps / t_s +
                          DRAM_BYTES_PER_SCORED_POSE * m["value"]) / 1e9 / peaks.get("hbm_gbs", 6650.0),
-            "brute_force_equivalent": {"tflops": brute, "frac": brute / fp32_peak,
+            "brute_force_equivalent": {"tflops": brute, "frac": brute / vec_peak,
                                        "work": "8 Nr Nl flops per scored pose"},
-            "issue_bound": {"warp_instructions_per_pair": WARP_INSTR_PER_PAIR,
-                            "ceiling_pairs_per_s": 148 * 4 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / WARP_INSTR_PER_PAIR,
-                            "frac": m["pairs_all"] / t_s /
-                                    (148 * 4 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / WARP_INSTR_PER_PAIR)},
             "per_scored_pose": {"pairs_in_cutoff": stats["pairs_in_cutoff"] / max(1, stats["scored_poses"]),
                                 "pairs_evaluated": stats["pairs_evaluated"] / max(1, stats["scored_poses"]),
                                 "pairs_brute_force": brute_pairs_per_pose(cfg)}}
+    if mixed:  # the mixed scorer's measured instruction count per in-cutoff pair
+        ceiling = 148 * 4 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / WARP_INSTR_PER_PAIR
+        out["issue_bound"] = {"warp_instructions_per_pair": WARP_INSTR_PER_PAIR, "ceiling_pairs_per_s": ceiling,
+                              "frac": m["pairs_all"] / t_s / ceiling}
+    return out
 
 
 def config_of(cfg, args):
@@ -680,7 +683,8 @@ def main():
     line = {
         "metric": METRIC, "value": m["value"], "unit": "scored poses/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "steps_per_s": args.steps / (t_ms / 1e3),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 pairs, f64 GSO",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f16/f32 pair tests, f64 table sums and GSO" if cfg["precision"] == "mixed" else "f64",
         "data": "synthetic (seeded globules, N(0,1) DFIRE table)", "config": config,
         "gpu_launches": 2 * args.steps,
         "e2e": {"value": es / (et / 1e3), "unit": "scored poses/s", "h2d_bytes_per_step": e2e["h2d"],

@@ -37,3 +37,22 @@ def test_work_per_pose_weighted_by_swarms():
     c1 = bench.CONFIGS["c1"]
     nr, nl, _ = c1["complexes"][0]
     assert bench.brute_pairs_per_pose(c1) == nr * nl
+
+
+def test_roofline_follows_the_precision():
+    """The roofline object rooflines a mixed run against the FP32 vector peak with the mixed scorer's
+    issue ceiling beside it, and an FP64 run against the FP64 vector peak without that ceiling."""
+    sys.path.insert(0, ROOT)
+    import argparse
+    import bench
+    m = {"run": {"stats": {"pairs_in_cutoff": 5.7e9, "pairs_evaluated": 2.7e10, "scored_poses": 1e5}},
+         "t_ms": 1000.0, "pairs_all": 5.7e9, "scored": 1e5, "value": 1e5}
+    args = argparse.Namespace(steps=10)
+    peaks = {"sm_max_mhz": 1965.0, "hbm_gbs": 7000.0}
+    for prec, bound, lanes in (("mixed", "fp32", 128), ("fp64", "fp64", 64)):
+        cfg = dict(bench.CONFIGS["c1"], precision=prec)
+        r = bench.roofline_of(cfg, "c1", m, args, peaks, "measured")
+        assert r["bound"] == bound
+        assert abs(r["peak"] - 148 * lanes * 2 * 1.965e9 / 1e12) < 1e-9
+        assert abs(r["achieved"] - 8 * 5.7e9 / 1e12) < 1e-12 and abs(r["frac"] - r["achieved"] / r["peak"]) < 1e-15
+        assert ("issue_bound" in r) == (prec == "mixed")
