@@ -55,9 +55,9 @@ L2_FLUSH_BYTES = 256 << 20
 # dram__bytes_read.sum + dram__bytes_write.sum of three launches (4,098 / 5,658 / 6,483 poses
 # rescored) on the 3002 / 1274-atom complex with 40 swarms: a fixed part (the L2-resident tables
 # and atom arrays read once per launch) plus a part per rescored pose (pose in, score and
-# reference point out), as summarised with the scorer's launch list under profiles/
-DRAM_BYTES_PER_LAUNCH = 9.52e6
-DRAM_BYTES_PER_SCORED_POSE = 144.0
+# reference point out), a least-squares fit, as summarised with the scorer's launch list under profiles/
+DRAM_BYTES_PER_LAUNCH = 9.12e6
+DRAM_BYTES_PER_SCORED_POSE = 212.0
 # warp-instructions the mixed scorer issues per receptor-ligand pair inside the cutoff, from ncu
 # smsp__inst_executed.sum of one launch (3002 / 1274 atoms, 4,098 poses, 233.9 M pairs in the
 # cutoff), as summarised with its full capture under profiles/; the scorer is issue-bound, so its
