@@ -60,9 +60,13 @@ DRAM_BYTES_PER_LAUNCH = 9.12e6
 DRAM_BYTES_PER_SCORED_POSE = 212.0
 # warp-instructions the mixed scorer issues per receptor-ligand pair inside the cutoff, from ncu
 # smsp__inst_executed.sum of one launch (3002 / 1274 atoms, 4,098 poses, 233.9 M pairs in the
-# cutoff), as summarised with its full capture under profiles/; the scorer is issue-bound, so its
-# ceiling is the SMs' issue rate (148 SMs x 4 schedulers x clock) over this count
+# cutoff), as summarised with its full capture under profiles/; one ceiling of the scorer is the
+# SMs' issue rate (148 SMs x 4 schedulers x clock) over this count
 WARP_INSTR_PER_PAIR = 5.96
+# L1 data-pipe wavefronts per in-cutoff pair in the same launch (l1tex__data_pipe_lsu_wavefronts:
+# 228.5 M shared-memory wavefronts plus ~181.6 M global-load ones, nearly all table gathers, over
+# 233.9 M pairs); the pipe retires one wavefront per SM per cycle, the other ceiling
+L1_WAVEFRONTS_PER_PAIR = 1.75
 
 
 def make_complexes(cfg, seed0=100):
@@ -558,10 +562,14 @@ def roofline_of(cfg, name, m, args, peaks, peak_src):
             "per_scored_pose": {"pairs_in_cutoff": stats["pairs_in_cutoff"] / max(1, stats["scored_poses"]),
                                 "pairs_evaluated": stats["pairs_evaluated"] / max(1, stats["scored_poses"]),
                                 "pairs_brute_force": brute_pairs_per_pose(cfg)}}
-    if mixed:  # the mixed scorer's measured instruction count per in-cutoff pair
-        ceiling = 148 * 4 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / WARP_INSTR_PER_PAIR
+    if mixed:  # the mixed scorer's measured instructions and L1 wavefronts per in-cutoff pair
+        clk = peaks.get("sm_max_mhz", 1965.0) * 1e6
+        ceiling = 148 * 4 * clk / WARP_INSTR_PER_PAIR
         out["issue_bound"] = {"warp_instructions_per_pair": WARP_INSTR_PER_PAIR, "ceiling_pairs_per_s": ceiling,
                               "frac": m["pairs_all"] / t_s / ceiling}
+        ceiling = 148 * clk / L1_WAVEFRONTS_PER_PAIR
+        out["l1_bound"] = {"wavefronts_per_pair": L1_WAVEFRONTS_PER_PAIR, "ceiling_pairs_per_s": ceiling,
+                           "frac": m["pairs_all"] / t_s / ceiling}
     return out
 
 

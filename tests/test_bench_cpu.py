@@ -55,4 +55,6 @@ def test_roofline_follows_the_precision():
         assert r["bound"] == bound
         assert abs(r["peak"] - 148 * lanes * 2 * 1.965e9 / 1e12) < 1e-9
         assert abs(r["achieved"] - 8 * 5.7e9 / 1e12) < 1e-12 and abs(r["frac"] - r["achieved"] / r["peak"]) < 1e-15
-        assert ("issue_bound" in r) == (prec == "mixed")
+        assert ("issue_bound" in r) == (prec == "mixed") and ("l1_bound" in r) == (prec == "mixed")
+        if prec == "mixed":
+            assert abs(r["l1_bound"]["ceiling_pairs_per_s"] - 148 * 1.965e9 / bench.L1_WAVEFRONTS_PER_PAIR) < 1.0
